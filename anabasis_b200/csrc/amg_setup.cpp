@@ -1,0 +1,209 @@
+// Aggregation AMG structure set-up (host).
+#include "amg_setup.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+namespace anb {
+namespace {
+
+// Plain CSR with diagonal separate; entry ids refer back to the fine storage for gathers.
+struct HCsr {
+  int n = 0;
+  std::vector<int> off, col;
+  std::vector<double> val, diag;
+};
+
+// One pass of pairwise matching; returns aggregate id per row and the aggregate count.
+std::vector<int> pairwise(const HCsr& A, double beta, int& nc) {
+  std::vector<int> agg(A.n, -1);
+  nc = 0;
+  for (int i = 0; i < A.n; ++i) {
+    if (agg[i] >= 0) continue;
+    double mx = 0.0;
+    for (int k = A.off[i]; k < A.off[i + 1]; ++k) mx = std::max(mx, -A.val[k]);
+    int best = -1;
+    double bestV = 0.0;
+    if (mx > 0.0) {
+      for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
+        const int j = A.col[k];
+        const double s = -A.val[k];
+        if (j == i || agg[j] >= 0 || s < beta * mx) continue;
+        if (best < 0 || s > bestV || (s == bestV && j < best)) {
+          best = j;
+          bestV = s;
+        }
+      }
+    }
+    agg[i] = nc;
+    if (best >= 0) agg[best] = nc;
+    ++nc;
+  }
+  return agg;
+}
+
+// Galerkin product with piecewise-constant prolongation.
+HCsr galerkin(const HCsr& A, const std::vector<int>& agg, int nc) {
+  HCsr C;
+  C.n = nc;
+  C.diag.assign(nc, 0.0);
+  std::vector<std::vector<std::pair<int, double>>> rows(nc);
+  for (int i = 0; i < A.n; ++i) {
+    const int I = agg[i];
+    C.diag[I] += A.diag[i];
+    for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
+      const int J = agg[A.col[k]];
+      if (J == I) {
+        C.diag[I] += A.val[k];
+        continue;
+      }
+      auto& r = rows[I];
+      auto it = std::find_if(r.begin(), r.end(), [J](const std::pair<int, double>& p) { return p.first == J; });
+      if (it == r.end()) r.push_back({J, A.val[k]});
+      else it->second += A.val[k];
+    }
+  }
+  C.off.assign(nc + 1, 0);
+  for (int I = 0; I < nc; ++I) {
+    std::sort(rows[I].begin(), rows[I].end());
+    C.off[I + 1] = C.off[I] + (int)rows[I].size();
+  }
+  C.col.resize(C.off[nc]);
+  C.val.resize(C.off[nc]);
+  for (int I = 0; I < nc; ++I)
+    for (size_t k = 0; k < rows[I].size(); ++k) {
+      C.col[C.off[I] + k] = rows[I][k].first;
+      C.val[C.off[I] + k] = rows[I][k].second;
+    }
+  return C;
+}
+
+void to_sell(const HCsr& A, AmgLevelHost& lv, std::vector<int>& csrToSell) {
+  lv.n = A.n;
+  lv.nSlices = (A.n + kSlice - 1) / kSlice;
+  lv.sliceOff.assign(lv.nSlices + 1, 0);
+  lv.rowLen.resize(A.n);
+  for (int i = 0; i < A.n; ++i) lv.rowLen[i] = A.off[i + 1] - A.off[i];
+  for (int s = 0; s < lv.nSlices; ++s) {
+    int w = 0;
+    for (int r = s * kSlice; r < std::min(A.n, (s + 1) * kSlice); ++r) w = std::max(w, lv.rowLen[r]);
+    lv.sliceOff[s + 1] = lv.sliceOff[s] + w * kSlice;
+  }
+  lv.col.assign(lv.sliceOff[lv.nSlices], 0);
+  csrToSell.assign(A.off[A.n], 0);
+  for (int s = 0; s < lv.nSlices; ++s) {
+    const int w = (lv.sliceOff[s + 1] - lv.sliceOff[s]) / kSlice;
+    for (int lane = 0; lane < kSlice; ++lane) {
+      const int r = s * kSlice + lane;
+      for (int k = 0; k < w; ++k) {
+        const int e = lv.sliceOff[s] + k * kSlice + lane;
+        if (r < A.n && k < lv.rowLen[r]) {
+          lv.col[e] = A.col[A.off[r] + k];
+          csrToSell[A.off[r] + k] = e;
+        } else {
+          lv.col[e] = r < A.n ? r : 0;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector<double>& vals,
+                                              const std::vector<double>& diag, const AmgSetupOptions& opt) {
+  std::vector<AmgLevelHost> levels;
+  // level 0 as CSR, remembering each CSR entry's SELL storage index
+  HCsr A;
+  A.n = L.nCells;
+  A.off.assign(A.n + 1, 0);
+  for (int r = 0; r < A.n; ++r) A.off[r + 1] = A.off[r] + L.rowLen[r];
+  A.col.resize(A.off[A.n]);
+  A.val.resize(A.off[A.n]);
+  A.diag = diag;
+  std::vector<int> storage(A.off[A.n]);
+  for (int r = 0; r < A.n; ++r) {
+    const int s = r / kSlice, lane = r % kSlice;
+    for (int k = 0; k < L.rowLen[r]; ++k) {
+      const int e = L.sliceOff[s] + k * kSlice + lane;
+      A.col[A.off[r] + k] = L.col[e];
+      A.val[A.off[r] + k] = vals[e];
+      storage[A.off[r] + k] = e;
+    }
+  }
+  {
+    AmgLevelHost lv0;
+    lv0.n = A.n;
+    lv0.nSlices = L.nSlices;
+    levels.push_back(std::move(lv0));  // pattern comes from the mesh layout
+  }
+  while ((int)levels.size() < opt.maxLevels && A.n > opt.coarseMax) {
+    // aggregates = composition of pairwise passes
+    std::vector<int> agg(A.n);
+    for (int i = 0; i < A.n; ++i) agg[i] = i;
+    int nc = A.n;
+    HCsr B = A;
+    for (int pass = 0; pass < opt.passesPerLevel; ++pass) {
+      int ncp = 0;
+      std::vector<int> a = pairwise(B, opt.strength, ncp);
+      for (int i = 0; i < A.n; ++i) agg[i] = a[agg[i]];
+      nc = ncp;
+      if (pass + 1 < opt.passesPerLevel) B = galerkin(B, a, ncp);
+    }
+    if (nc > (int)(0.9 * A.n) || nc < 1) break;  // coarsening stalled
+    HCsr Cc = galerkin(A, agg, nc);
+    AmgLevelHost& fine = levels.back();
+    fine.nc = nc;
+    fine.agg = agg;
+    fine.memOff.assign(nc + 1, 0);
+    for (int i = 0; i < A.n; ++i) fine.memOff[agg[i] + 1]++;
+    for (int I = 0; I < nc; ++I) fine.memOff[I + 1] += fine.memOff[I];
+    fine.mem.assign(A.n, 0);
+    {
+      std::vector<int> fill(fine.memOff.begin(), fine.memOff.end() - 1);
+      for (int i = 0; i < A.n; ++i) fine.mem[fill[agg[i]]++] = i;
+    }
+    AmgLevelHost coarse;
+    std::vector<int> cCsrToSell;
+    to_sell(Cc, coarse, cCsrToSell);
+    // gather lists: coarse SELL entries then coarse diagonals
+    const int nEnt = coarse.sliceOff[coarse.nSlices];
+    std::vector<int> cnt(nEnt + nc + 1, 0);
+    std::vector<int> target(A.off[A.n]);
+    for (int i = 0; i < A.n; ++i) {
+      const int I = agg[i];
+      for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
+        const int J = agg[A.col[k]];
+        int t;
+        if (J == I) t = nEnt + I;
+        else {
+          const int* b = &Cc.col[Cc.off[I]];
+          const int* e = &Cc.col[Cc.off[I + 1]];
+          const int* it = std::lower_bound(b, e, J);
+          t = cCsrToSell[Cc.off[I] + (int)(it - &Cc.col[0]) - Cc.off[I]];
+        }
+        target[k] = t;
+        cnt[t + 1]++;
+      }
+      cnt[nEnt + I + 1]++;  // fine diagonal
+    }
+    fine.gOff.assign(nEnt + nc + 1, 0);
+    for (int t = 0; t < nEnt + nc; ++t) fine.gOff[t + 1] = fine.gOff[t] + cnt[t + 1];
+    fine.gIdx.assign(fine.gOff.back(), 0);
+    {
+      std::vector<int> fill(fine.gOff.begin(), fine.gOff.end() - 1);
+      for (int i = 0; i < A.n; ++i) {
+        for (int k = A.off[i]; k < A.off[i + 1]; ++k) fine.gIdx[fill[target[k]]++] = storage[k];
+        fine.gIdx[fill[nEnt + agg[i]]++] = -1 - i;
+      }
+    }
+    levels.push_back(std::move(coarse));
+    // next level's CSR with storage indices of the coarse SELL
+    A = std::move(Cc);
+    storage = cCsrToSell;
+  }
+  return levels;
+}
+
+}  // namespace anb

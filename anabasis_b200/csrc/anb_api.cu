@@ -1,0 +1,1001 @@
+// C ABI of libanb.so: context, device memory, SIMPLE orchestration (include/anb.h).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/anb.h"
+#include "amg_setup.hpp"
+#include "host_mesh.hpp"
+#include "kernels.cuh"
+#include "layout.hpp"
+
+namespace anb {
+
+struct AnbError : std::runtime_error {
+  int code;
+  AnbError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                                          \
+  do {                                                                                                    \
+    cudaError_t e_ = (call);                                                                              \
+    if (e_ != cudaSuccess)                                                                                \
+      throw AnbError(ANB_ERR_CUDA, std::string("CUDA error ") + cudaGetErrorString(e_) + " at " #call);   \
+  } while (0)
+
+// Device allocations owned by a context; freed together.
+class DevArena {
+ public:
+  ~DevArena() { release(); }
+  template <class T>
+  T* alloc(size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    ptrs_.push_back(p);
+    bytes_ += n * sizeof(T);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& h) {
+    T* d = alloc<T>(h.size());
+    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+  }
+  void release() {
+    for (void* p : ptrs_) cudaFree(p);
+    ptrs_.clear();
+    bytes_ = 0;
+  }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  std::vector<void*> ptrs_;
+  size_t bytes_ = 0;
+};
+
+}  // namespace anb
+
+using namespace anb;
+
+struct anb_ctx {
+  std::string err;
+  anb_params prm{};
+  HostMesh hm;
+  Layout L;
+  int C = 0, nI = 0, nB = 0, nEnt = 0;
+  cudaStream_t stream = nullptr;
+  LaunchCfg lc{};
+  DevArena arena, amgArena;
+  DMesh dm{};
+  // face-slot lookup for diagnostics: storage entry of (owner row, neighbour col) and back
+  std::vector<int> slotOwn, slotNei;
+  // device buffers
+  FaceRec* dFace = nullptr;
+  BndRec* dBnd = nullptr;
+  uint8_t* dBType = nullptr;
+  double* dBVal = nullptr;
+  double *dBA = nullptr, *dBN = nullptr;
+  double *U = nullptr, *Us = nullptr, *P = nullptr, *Pc = nullptr, *rau = nullptr;
+  double *G = nullptr, *Gc = nullptr;
+  double *mval = nullptr, *mdiag = nullptr, *rhs = nullptr;
+  double *pval = nullptr, *pdiag = nullptr, *pb = nullptr, *divStar = nullptr, *divCorr = nullptr;
+  double *phiStar = nullptr, *phi = nullptr;
+  double *bw[8] = {nullptr};  // BiCGSTAB work vectors (3*C each)
+  double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pq = nullptr, *pdx = nullptr;
+  double* scal = nullptr;     // device scalars
+  int* flags = nullptr;
+  double* stats = nullptr;
+  double* forceOut = nullptr;
+  Reducer red{};
+  // pinned host mirrors
+  int* hFlags = nullptr;
+  double* hScal = nullptr;
+  // state
+  bool bcSet = false, stateSet = false, pZeroBC = true;
+  long long outerStep = 0;
+  int lastMomIts = 8, lastPIts = 8;
+  // AMG
+  bool amgBuilt = false;
+  AmgDev amg;
+  std::vector<AmgLevelHost> amgHost;
+};
+
+namespace {
+
+// Message of the last failed anb_create on this thread (anb_last_error(NULL)).
+thread_local std::string g_createError = "no context";
+
+int fail(anb_ctx* c, const AnbError& e) {
+  if (c) c->err = e.what();
+  return e.code;
+}
+
+template <class F>
+int guarded(anb_ctx* c, F&& f) {
+  try {
+    return f();
+  } catch (const AnbError& e) {
+    return fail(c, e);
+  } catch (const std::bad_alloc&) {
+    if (c) c->err = "host allocation failed";
+    return ANB_ERR_INVALID;
+  } catch (const std::exception& e) {
+    if (c) c->err = e.what();
+    return ANB_ERR_MESH;
+  }
+}
+
+constexpr int kScalBicg = 0;    // 3 * 8
+constexpr int kScalPcg = 24;    // 8
+constexpr int kFlagBicg = 0;    // 3 * 4
+constexpr int kFlagPcg = 12;    // 4
+
+void permute_in(const anb_ctx* c, const double* src, std::vector<double>& dst, int comps) {
+  dst.resize((size_t)comps * c->C);
+  for (int q = 0; q < comps; ++q)
+    for (int r = 0; r < c->C; ++r) dst[(size_t)q * c->C + r] = src[(size_t)q * c->C + c->L.new2old[r]];
+}
+
+void upload_cells(anb_ctx* c, const double* const* src, double* dst, int comps) {
+  std::vector<double> h((size_t)comps * c->C);
+  for (int q = 0; q < comps; ++q)
+    for (int r = 0; r < c->C; ++r) h[(size_t)q * c->C + r] = src[q][c->L.new2old[r]];
+  CK(cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+void download_cells(anb_ctx* c, const double* src, double* const* dst, int comps) {
+  std::vector<double> h((size_t)comps * c->C);
+  CK(cudaMemcpyAsync(h.data(), src, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < comps; ++q)
+    if (dst[q])
+      for (int r = 0; r < c->C; ++r) dst[q][c->L.new2old[r]] = h[(size_t)q * c->C + r];
+}
+
+// Face array on the device (new order, new orientation) -> input order and orientation.
+void download_faces(anb_ctx* c, const double* src, double* dst) {
+  const int nF = c->nI + c->nB;
+  std::vector<double> h(nF);
+  CK(cudaMemcpyAsync(h.data(), src, nF * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int fi = 0; fi < c->nI; ++fi) dst[c->L.fOrig[fi]] = c->L.fFlip[fi] ? -h[fi] : h[fi];
+  for (int b = 0; b < c->nB; ++b) dst[c->nI + b] = h[c->nI + b];
+}
+
+// Off-diagonal matrix values per input face in input orientation.
+void download_offdiag(anb_ctx* c, const double* val, double* a_pn, double* a_np) {
+  std::vector<double> h(c->nEnt);
+  CK(cudaMemcpyAsync(h.data(), val, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int fi = 0; fi < c->nI; ++fi) {
+    const double own = h[c->slotOwn[fi]], nei = h[c->slotNei[fi]];
+    const int f = c->L.fOrig[fi];
+    const bool flip = c->L.fFlip[fi] != 0;
+    if (a_pn) a_pn[f] = flip ? nei : own;
+    if (a_np) a_np[f] = flip ? own : nei;
+  }
+}
+
+DSell mom_sell(const anb_ctx* c) { return DSell{c->C, c->L.sliceOff.empty() ? nullptr : c->dm.sliceOff, c->dm.col, c->mval, c->mdiag}; }
+DSell p_sell(const anb_ctx* c) { return DSell{c->C, c->dm.sliceOff, c->dm.col, c->pval, c->pdiag}; }
+
+void grad(anb_ctx* c, int nf, const double* const* phi, const unsigned char* bits, double* const* out) {
+  GradArgs a{};
+  a.nf = nf;
+  for (int f = 0; f < nf; ++f) {
+    a.phi[f] = phi[f];
+    a.bit[f] = bits[f];
+    const int q = bits[f] == 1 ? 0 : bits[f] == 2 ? 1 : bits[f] == 4 ? 2 : 3;
+    a.bval[f] = c->dBVal + (size_t)q * c->nB;
+    a.g[f] = out[f];
+  }
+  launch_lsq_grad(c->lc, c->dm, a);
+}
+
+void poll(anb_ctx* c, const int* dflags, int count) {
+  CK(cudaMemcpyAsync(c->hFlags, dflags, sizeof(int) * count, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+// Momentum: nc-component BiCGSTAB + Jacobi on the shared matrix; comps with active[q]==0 are
+// frozen.  Returns per-component iterations and convergence.
+void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
+  BicgArgs a{};
+  a.A = mom_sell(c);
+  a.nc = 3;
+  a.b = c->rhs;
+  a.x = c->Us;
+  a.r = c->bw[0]; a.rh = c->bw[1]; a.p = c->bw[2]; a.v = c->bw[3];
+  a.s = c->bw[4]; a.t = c->bw[5]; a.ph = c->bw[6]; a.sh = c->bw[7];
+  a.sc = c->scal + kScalBicg;
+  a.fl = c->flags + kFlagBicg;
+  a.atol = c->prm.vel_tol;
+  a.rtol = c->prm.vel_rel_tol;
+  a.maxit = c->prm.vel_maxit;
+  a.red = c->red;
+  bicg_init(c->lc, a);
+  // freeze inactive components
+  for (int q = 0; q < 3; ++q)
+    if (!active[q]) {
+      const int one[4] = {1, 0, 0, 1};
+      CK(cudaMemcpyAsync(a.fl + 4 * q, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
+    }
+  int done = 0;
+  int batch = std::max(2, std::min(c->lastMomIts, 32));
+  while (true) {
+    for (int k = 0; k < batch; ++k) bicg_iteration(c->lc, a);
+    done += batch;
+    poll(c, a.fl, 12);
+    bool all = true;
+    for (int q = 0; q < 3; ++q) all = all && c->hFlags[4 * q];
+    if (all || done > a.maxit + 2) break;
+    batch = 4;
+  }
+  int mx = 0;
+  for (int q = 0; q < 3; ++q) {
+    its[q] = active[q] ? c->hFlags[4 * q + 2] : 0;
+    conv[q] = active[q] ? c->hFlags[4 * q + 3] != 0 : true;
+    mx = std::max(mx, its[q]);
+  }
+  c->lastMomIts = std::max(1, mx);
+}
+
+void ensure_amg(anb_ctx* c);
+
+// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
+void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  PcgArgs a{};
+  a.A = p_sell(c);
+  a.b = b;
+  a.x = x;
+  a.r = c->pr; a.z = c->pz; a.p0 = c->pp0; a.p1 = c->pp1; a.q = c->pq;
+  a.sc = c->scal + kScalPcg;
+  a.fl = c->flags + kFlagPcg;
+  a.atol = c->prm.p_tol;
+  a.rtol = rtol;
+  a.maxit = c->prm.p_maxit;
+  a.red = c->red;
+  const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
+  if (amg) c->amg.lv[0].b = c->pr;
+  pcg_init(c->lc, a);
+  pcg_precondition(c->lc, a, amg);
+  int it = 0;
+  int batch = std::max(2, std::min(c->lastPIts, 64));
+  while (true) {
+    for (int k = 0; k < batch; ++k) pcg_iteration(c->lc, a, it++, amg);
+    poll(c, a.fl, 4);
+    if (c->hFlags[0] || it > a.maxit + 2) break;
+    batch = std::max(2, std::min(8, batch / 2 + 1));
+  }
+  *its = c->hFlags[1];
+  *conv = c->hFlags[2] != 0;
+  c->lastPIts = std::max(1, *its);
+}
+
+void ensure_amg(anb_ctx* c) {
+  if (!c->prm.p_use_amg) return;
+  if (!c->amgBuilt) {
+    std::vector<double> hv(c->nEnt), hd(c->C);
+    CK(cudaMemcpyAsync(hv.data(), c->pval, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hd.data(), c->pdiag, hd.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    AmgSetupOptions opt;
+    c->amgHost = build_amg_hierarchy(c->L, hv, hd, opt);
+    AmgDev& A = c->amg;
+    A.nLevels = (int)c->amgHost.size();
+    DevArena& ar = c->amgArena;
+    for (int l = 0; l < A.nLevels; ++l) {
+      const AmgLevelHost& h = c->amgHost[l];
+      AmgLevelDev& d = A.lv[l];
+      d = AmgLevelDev{};
+      d.n = h.n;
+      d.nc = h.nc;
+      if (l == 0) {
+        d.sliceOff = c->dm.sliceOff;
+        d.col = c->dm.col;
+        d.val = c->pval;
+        d.diag = c->pdiag;
+      } else {
+        d.sliceOff = ar.upload(h.sliceOff);
+        d.col = ar.upload(h.col);
+        d.val = ar.alloc<double>(h.sliceOff.back());
+        d.diag = ar.alloc<double>(h.n);
+        d.b = ar.alloc<double>(h.n);
+      }
+      d.x = ar.alloc<double>(h.n);
+      d.x2 = ar.alloc<double>(h.n);
+      if (l + 1 < A.nLevels) {
+        d.agg = ar.upload(h.agg);
+        d.memOff = ar.upload(h.memOff);
+        d.mem = ar.upload(h.mem);
+        d.gOff = ar.upload(h.gOff);
+        d.gIdx = ar.upload(h.gIdx);
+        d.nEntNext = c->amgHost[l + 1].sliceOff.back();
+      }
+    }
+    const int nd = c->amgHost.back().n;
+    if (nd > 160) throw AnbError(ANB_ERR_UNSUPPORTED, "AMG coarsest level too large (" + std::to_string(nd) + ")");
+    A.nDense = nd;
+    A.dense = ar.alloc<double>((size_t)nd * nd);
+    c->amgBuilt = true;
+  }
+  if (c->amg.nLevels >= 2) amg_refresh(c->lc, c->amg);
+}
+
+void check_ready(anb_ctx* c) {
+  if (!c->bcSet) throw AnbError(ANB_ERR_INVALID, "boundary conditions not set (anb_set_bc)");
+  if (!c->stateSet) throw AnbError(ANB_ERR_INVALID, "state not set (anb_set_state)");
+  CK(cudaSetDevice(c->prm.device));
+}
+
+// One SIMPLE outer iteration, main.cu:3388-3634.
+int simple_step(anb_ctx* c, anb_iter_stats* st) {
+  const int C = c->C;
+  const anb_params& p = c->prm;
+  bool anyNC = false;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  ++c->outerStep;
+  // 1. gradients of the old fields (u, v, w with their BC sets, p)
+  {
+    const double* phi[4] = {c->U, c->U + C, c->U + 2 * C, c->P};
+    const unsigned char bits[4] = {1, 2, 4, 8};
+    double* out[4] = {c->G, c->G + 3 * C, c->G + 6 * C, c->G + 9 * C};
+    grad(c, 4, phi, bits, out);
+  }
+  // 2. momentum matrix (u pass) + three right-hand sides + relaxation + rAU
+  MomArgs ma{};
+  ma.U = c->U;
+  ma.Q = c->U;
+  ma.G = c->G;
+  ma.rho = p.rho;
+  ma.mu = p.mu;
+  ma.uRelax = p.u_relax;
+  ma.relax = p.u_relax < 0.999999 ? 1 : 0;
+  ma.rhsOnly = 0;
+  ma.val = c->mval;
+  ma.diag = c->mdiag;
+  ma.rhs = c->rhs;
+  ma.rau = c->rau;
+  launch_momentum(c->lc, c->dm, ma);
+  CK(cudaMemcpyAsync(c->Us, c->U, sizeof(double) * 3 * C, cudaMemcpyDeviceToDevice, c->stream));
+  int its[3] = {0, 0, 0};
+  {
+    const int nVel = std::max(p.n_vel_nonorth_corr, 0) + 1;
+    int active[3] = {1, 1, 1};
+    std::vector<double> qPrev;
+    for (int it = 1; it <= nVel; ++it) {
+      if (it > 1) {
+        // rhs-only re-assembly on the current iterates (K26, K9, K7, K8, K10)
+        const double* phi[3] = {c->Us, c->Us + C, c->Us + 2 * C};
+        const unsigned char bits[3] = {1, 2, 4};
+        double* out[3] = {c->G, c->G + 3 * C, c->G + 6 * C};
+        grad(c, 3, phi, bits, out);
+        MomArgs mr = ma;
+        mr.Q = c->Us;
+        mr.rhsOnly = 1;
+        launch_momentum(c->lc, c->dm, mr);
+      }
+      // keep the iterate for the relative-change test (main.cu:3377-3381)
+      std::vector<double> before;
+      if (nVel > 1) {
+        before.resize((size_t)3 * C);
+        CK(cudaMemcpyAsync(before.data(), c->Us, sizeof(double) * 3 * C, cudaMemcpyDeviceToHost, c->stream));
+      }
+      int itq[3];
+      bool cv[3];
+      solve_momentum(c, active, itq, cv);
+      for (int q = 0; q < 3; ++q)
+        if (active[q]) {
+          its[q] = itq[q];
+          anyNC = anyNC || !cv[q];
+        }
+      if (nVel > 1 && it < nVel) {
+        std::vector<double> after((size_t)3 * C);
+        CK(cudaMemcpyAsync(after.data(), c->Us, sizeof(double) * 3 * C, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int q = 0; q < 3; ++q) {
+          if (!active[q]) continue;
+          double num = 0.0, den = 1.0;
+          for (int r = 0; r < C; ++r) {
+            const double d = after[(size_t)q * C + r] - before[(size_t)q * C + r];
+            num += d * d;
+            den += after[(size_t)q * C + r] * after[(size_t)q * C + r];
+          }
+          if (std::sqrt(num / den) < p.corr_tol) active[q] = 0;
+        }
+        if (!active[0] && !active[1] && !active[2]) break;
+      }
+    }
+  }
+  // 3. pressure matrix + Rhie-Chow flux + continuity, p' = 0
+  PresArgs pa{};
+  pa.Us = c->Us;
+  pa.P = c->P;
+  pa.Gp = c->G + 9 * C;
+  pa.rau = c->rau;
+  pa.rho = p.rho;
+  pa.val = c->pval;
+  pa.diag = c->pdiag;
+  pa.phiStar = c->phiStar;
+  pa.divStar = c->divStar;
+  pa.b = c->pb;
+  pa.pc = c->Pc;
+  launch_pressure_rc(c->lc, c->dm, pa);
+  const int every = std::max(p.p_amg_rebuild_every, 1);
+  if (!c->amgBuilt || c->outerStep == 1 || ((c->outerStep - 1) % every) == 0) ensure_amg(c);
+  // 4. non-orthogonal pressure passes
+  const int nPS = std::max(p.n_nonorth_corr, 0) + 1, nExtra = std::max(p.n_pressure_corr, 0);
+  const int total = nPS + nExtra;
+  int counter = 0, pTot = 0, pLast = 0;
+  NonOrthArgs na{c->rau, c->Gc, c->divStar, c->pb};
+  FluxArgs fa{};
+  fa.rau = c->rau;
+  fa.Gc = c->Gc;
+  fa.pc = c->Pc;
+  fa.phiStar = c->phiStar;
+  fa.phi = c->phi;
+  fa.divCorr = c->divCorr;
+  fa.pRelax = p.p_relax;
+  fa.P = c->P;
+  fa.U = c->U;
+  fa.Us = c->Us;
+  fa.red = c->red;
+  fa.stats = c->stats;
+  const unsigned char pbit[1] = {8};
+  for (int pc = 1; pc <= nPS; ++pc) {
+    if (pc > 1 || !c->pZeroBC) {
+      const double* phi[1] = {c->Pc};
+      double* out[1] = {c->Gc};
+      grad(c, 1, phi, pbit, out);
+      launch_nonorth_rhs(c->lc, c->dm, na);
+    }
+    ++counter;
+    const double rtol = counter == total ? 0.0 : p.p_rel_tol;
+    bool cv = true;
+    solve_pressure(c, c->pb, c->Pc, rtol, &pLast, &cv);
+    anyNC = anyNC || !cv;
+    pTot += pLast;
+    if (pc == nPS) {
+      const double* phi[1] = {c->Pc};
+      double* out[1] = {c->Gc};
+      grad(c, 1, phi, pbit, out);
+      fa.update = nExtra == 0 ? 1 : 0;
+      launch_flux_final(c->lc, c->dm, fa);
+    }
+  }
+  for (int k = 1; k <= nExtra; ++k) {  // main.cu:3521-3567
+    // b = -divCorr ; dp' from zero ; p' += dp'
+    std::vector<double> h(C);
+    CK(cudaMemcpyAsync(h.data(), c->divCorr, sizeof(double) * C, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (double& v : h) v = -v;
+    CK(cudaMemcpyAsync(c->pb, h.data(), sizeof(double) * C, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(c->pdx, 0, sizeof(double) * C, c->stream));
+    ++counter;
+    const double rtol = counter == total ? 0.0 : p.p_rel_tol;
+    bool cv = true;
+    solve_pressure(c, c->pb, c->pdx, rtol, &pLast, &cv);
+    anyNC = anyNC || !cv;
+    pTot += pLast;
+    std::vector<double> hp(C), hd(C);
+    CK(cudaMemcpyAsync(hp.data(), c->Pc, sizeof(double) * C, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hd.data(), c->pdx, sizeof(double) * C, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int r = 0; r < C; ++r) hp[r] += 1.0 * hd[r];
+    CK(cudaMemcpyAsync(c->Pc, hp.data(), sizeof(double) * C, cudaMemcpyHostToDevice, c->stream));
+    const double* phi[1] = {c->Pc};
+    double* out[1] = {c->Gc};
+    grad(c, 1, phi, pbit, out);
+    fa.update = k == nExtra ? 1 : 0;
+    launch_flux_final(c->lc, c->dm, fa);
+  }
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaMemcpyAsync(c->hScal, c->stats, sizeof(double) * 9, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  const double* s = c->hScal;
+  st->mass_res = s[8];
+  st->du_rel = std::sqrt(s[0] / (1.0 + s[1]));
+  st->dv_rel = std::sqrt(s[2] / (1.0 + s[3]));
+  st->dw_rel = std::sqrt(s[4] / (1.0 + s[5]));
+  st->dp_rel = std::sqrt(s[6] / (1.0 + s[7]));
+  st->its_u = its[0];
+  st->its_v = its[1];
+  st->its_w = its[2];
+  st->its_p_last = pLast;
+  st->its_p_total = pTot;
+  st->iter_seconds = ms * 1e-3;
+  st->status = anyNC ? ANB_NOT_CONVERGED : ANB_OK;
+  return st->status;
+}
+
+void build_slot_lookup(anb_ctx* c) {
+  c->slotOwn.assign(c->nI, -1);
+  c->slotNei.assign(c->nI, -1);
+  for (int s = 0; s < c->L.nSlices; ++s) {
+    const int w = (c->L.sliceOff[s + 1] - c->L.sliceOff[s]) / kSlice;
+    for (int lane = 0; lane < kSlice; ++lane) {
+      const int r = s * kSlice + lane;
+      if (r >= c->C) continue;
+      for (int k = 0; k < w; ++k) {
+        const int e = c->L.sliceOff[s] + k * kSlice + lane;
+        const int f = c->L.slotFace[e];
+        if (f < 0) continue;
+        if (c->L.fOwner[f] == r) c->slotOwn[f] = e;
+        else c->slotNei[f] = e;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void anb_default_params(anb_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->rho = 1.0;
+  p->mu = 0.05;
+  p->u_relax = 0.7;
+  p->p_relax = 1.0;
+  p->n_nonorth_corr = 2;
+  p->n_vel_nonorth_corr = 0;
+  p->n_pressure_corr = 0;
+  p->vel_maxit = 100;
+  p->vel_tol = 1e-10;
+  p->vel_rel_tol = 0.0;
+  p->p_maxit = 4000;
+  p->p_tol = 1e-10;
+  p->p_rel_tol = 0.0;
+  p->corr_tol = 1e-12;
+  p->p_amg_rebuild_every = 1;
+  p->p_use_amg = 1;
+  p->precision = ANB_PRECISION_FP64;
+  p->device = 0;
+}
+
+const char* anb_last_error(const anb_ctx* c) { return c ? c->err.c_str() : g_createError.c_str(); }
+
+int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
+  if (!out) return ANB_ERR_INVALID;
+  *out = nullptr;
+  if (!md || !prm) return ANB_ERR_INVALID;
+  auto c = std::make_unique<anb_ctx>();
+  int rc = guarded(c.get(), [&]() -> int {
+    c->prm = *prm;
+    if (prm->precision != ANB_PRECISION_FP64 && prm->precision != ANB_PRECISION_MIXED)
+      throw AnbError(ANB_ERR_INVALID, "unknown precision");
+    if (md->n_points <= 0 || md->n_faces <= 0 || md->n_internal_faces < 0 || md->n_internal_faces > md->n_faces ||
+        !md->points || !md->face_offsets || !md->face_points || !md->owner ||
+        (md->n_internal_faces > 0 && !md->neighbour) || md->n_patches < 0)
+      throw AnbError(ANB_ERR_INVALID, "invalid mesh description");
+    HostMesh& m = c->hm;
+    m.points.resize(md->n_points);
+    for (int i = 0; i < md->n_points; ++i)
+      m.points[i] = {md->points[3 * i], md->points[3 * i + 1], md->points[3 * i + 2]};
+    m.faceOff.assign(md->face_offsets, md->face_offsets + md->n_faces + 1);
+    if (m.faceOff[0] != 0) throw AnbError(ANB_ERR_INVALID, "face_offsets must start at 0");
+    for (int f = 0; f < md->n_faces; ++f)
+      if (m.faceOff[f + 1] - m.faceOff[f] < 3) throw AnbError(ANB_ERR_MESH, "face " + std::to_string(f) + " has fewer than 3 points");
+    m.facePts.assign(md->face_points, md->face_points + m.faceOff.back());
+    m.owner.assign(md->owner, md->owner + md->n_faces);
+    m.neigh.assign(md->neighbour, md->neighbour + md->n_internal_faces);
+    m.patches.resize(md->n_patches);
+    std::vector<int> cover(md->n_faces, 0);
+    for (int k = 0; k < md->n_patches; ++k) {
+      m.patches[k].start = md->patch_start[k];
+      m.patches[k].nFaces = md->patch_size[k];
+      m.patches[k].name = "patch" + std::to_string(k);
+      if (md->patch_size[k] < 0 || md->patch_start[k] < md->n_internal_faces ||
+          md->patch_start[k] + md->patch_size[k] > md->n_faces)
+        throw AnbError(ANB_ERR_MESH, "patch " + std::to_string(k) + " has an invalid face range");
+      for (int f = md->patch_start[k]; f < md->patch_start[k] + md->patch_size[k]; ++f) cover[f]++;
+    }
+    for (int f = md->n_internal_faces; f < md->n_faces; ++f)
+      if (cover[f] != 1) throw AnbError(ANB_ERR_MESH, "boundary face " + std::to_string(f) + " is not in exactly one patch");
+    finalize_topology(m);
+    for (int v : m.owner)
+      if (v < 0) throw AnbError(ANB_ERR_MESH, "negative owner label");
+    compute_geometry(m);
+    c->L = build_layout(m);
+    Layout& L = c->L;
+    c->C = L.nCells;
+    c->nI = L.nInternal;
+    c->nB = L.nBoundary;
+    c->nEnt = L.sliceOff.back();
+    build_slot_lookup(c.get());
+
+    CK(cudaSetDevice(prm->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int nSM = 148;
+    CK(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, prm->device));
+    c->lc.stream = c->stream;
+    c->lc.rowBlocks = std::max(1, std::min((c->C + kBlock - 1) / kBlock, nSM * 8));
+
+    DevArena& A = c->arena;
+    // faces
+    std::vector<FaceRec> fr(c->nI);
+    for (int f = 0; f < c->nI; ++f) {
+      fr[f].lam = L.fLam[f];
+      fr[f].g = L.fG[f];
+      for (int k = 0; k < 3; ++k) {
+        fr[f].t[k] = L.fT[3 * f + k];
+        fr[f].d[k] = L.fD[3 * f + k];
+      }
+    }
+    std::vector<BndRec> br(c->nB);
+    std::vector<double> bA(c->nB), bN((size_t)3 * c->nB);
+    for (int b = 0; b < c->nB; ++b) {
+      const int f = c->nI + b;
+      br[b].g = L.bG[b];
+      for (int k = 0; k < 3; ++k) {
+        br[b].t[k] = L.bT[3 * b + k];
+        br[b].S[k] = L.bS[3 * b + k];
+        br[b].d[k] = m.xf[f][k] - m.cc[m.owner[f]][k];
+        bN[3 * b + k] = m.nf[f][k];
+      }
+      bA[b] = m.Af[f];
+    }
+    c->dFace = A.upload(fr);
+    c->dBnd = A.upload(br);
+    c->dBA = A.upload(bA);
+    c->dBN = A.upload(bN);
+    c->dBType = A.alloc<uint8_t>(c->nB);
+    c->dBVal = A.alloc<double>((size_t)4 * c->nB);
+    DMesh& dm = c->dm;
+    dm.nCells = c->C;
+    dm.nInternal = c->nI;
+    dm.nBoundary = c->nB;
+    dm.nSlices = L.nSlices;
+    dm.sliceOff = A.upload(L.sliceOff);
+    dm.col = A.upload(L.col);
+    dm.slotFace = A.upload(L.slotFace);
+    dm.face = c->dFace;
+    dm.fFlags = A.upload(L.fFlags);
+    dm.bOwner = A.upload(L.bOwner);
+    dm.bnd = c->dBnd;
+    dm.bFlags = A.upload(L.bFlags);
+    dm.cbOff = A.upload(L.cbOff);
+    dm.cbList = A.upload(L.cbList);
+    dm.vol = A.upload(L.vol);
+    dm.cc = A.upload(L.cc);
+    dm.minv = A.upload(L.minv);
+    dm.bType = c->dBType;
+    dm.bVal = c->dBVal;
+    // fields and work
+    const size_t C = c->C, F = (size_t)c->nI + c->nB;
+    c->U = A.alloc<double>(3 * C);
+    c->Us = A.alloc<double>(3 * C);
+    c->P = A.alloc<double>(C);
+    c->Pc = A.alloc<double>(C);
+    c->rau = A.alloc<double>(C);
+    c->G = A.alloc<double>(12 * C);
+    c->Gc = A.alloc<double>(3 * C);
+    c->mval = A.alloc<double>(c->nEnt);
+    c->mdiag = A.alloc<double>(C);
+    c->rhs = A.alloc<double>(3 * C);
+    c->pval = A.alloc<double>(c->nEnt);
+    c->pdiag = A.alloc<double>(C);
+    c->pb = A.alloc<double>(C);
+    c->divStar = A.alloc<double>(C);
+    c->divCorr = A.alloc<double>(C);
+    c->phiStar = A.alloc<double>(F);
+    c->phi = A.alloc<double>(F);
+    for (int k = 0; k < 8; ++k) c->bw[k] = A.alloc<double>(3 * C);
+    c->pr = A.alloc<double>(C);
+    c->pz = A.alloc<double>(C);
+    c->pp0 = A.alloc<double>(C);
+    c->pp1 = A.alloc<double>(C);
+    c->pq = A.alloc<double>(C);
+    c->pdx = A.alloc<double>(C);
+    c->scal = A.alloc<double>(64);
+    c->flags = A.alloc<int>(32);
+    c->stats = A.alloc<double>(16);
+    c->forceOut = A.alloc<double>(16);
+    c->red.partials = A.alloc<double>((size_t)(nSM * 8 + 16) * 16);
+    c->red.ticket = A.alloc<unsigned int>(1);
+    CK(cudaMemset(c->red.ticket, 0, sizeof(unsigned int)));
+    CK(cudaMemset(c->mval, 0, sizeof(double) * c->nEnt));
+    CK(cudaMemset(c->pval, 0, sizeof(double) * c->nEnt));
+    CK(cudaMemset(c->phi, 0, sizeof(double) * F));
+    CK(cudaMemset(c->Pc, 0, sizeof(double) * C));
+    CK(cudaMallocHost(&c->hFlags, sizeof(int) * 32));
+    CK(cudaMallocHost(&c->hScal, sizeof(double) * 64));
+    return ANB_OK;
+  });
+  if (rc != ANB_OK) {
+    g_createError = c->err;
+    c->arena.release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->hFlags) cudaFreeHost(c->hFlags);
+    if (c->hScal) cudaFreeHost(c->hScal);
+    return rc;
+  }
+  *out = c.release();
+  return ANB_OK;
+}
+
+void anb_destroy(anb_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->prm.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->amgArena.release();
+  c->arena.release();
+  if (c->hFlags) cudaFreeHost(c->hFlags);
+  if (c->hScal) cudaFreeHost(c->hScal);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int anb_get_sizes(const anb_ctx* c, int* nc, int* nf, int* ni, int* np) {
+  if (!c) return ANB_ERR_INVALID;
+  if (nc) *nc = c->C;
+  if (nf) *nf = c->nI + c->nB;
+  if (ni) *ni = c->nI;
+  if (np) *np = (int)c->hm.patches.size();
+  return ANB_OK;
+}
+
+int anb_get_geometry(anb_ctx* c, double* cc, double* vol, double* xf, double* nf, double* area, double* mx) {
+  if (!c) return ANB_ERR_INVALID;
+  const HostMesh& m = c->hm;
+  for (int i = 0; i < m.nCells; ++i) {
+    if (cc) for (int k = 0; k < 3; ++k) cc[3 * i + k] = m.cc[i][k];
+    if (vol) vol[i] = m.vol[i];
+  }
+  for (int f = 0; f < m.nFaces; ++f) {
+    for (int k = 0; k < 3; ++k) {
+      if (xf) xf[3 * f + k] = m.xf[f][k];
+      if (nf) nf[3 * f + k] = m.nf[f][k];
+    }
+    if (area) area[f] = m.Af[f];
+  }
+  if (mx) *mx = m.maxNonOrthDeg;
+  return ANB_OK;
+}
+
+int anb_set_bc(anb_ctx* c, const int* tu, const int* tv, const int* tw, const int* tp, const double* uf,
+               const double* vf, const double* wf, const double* pf) {
+  if (!c) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    if (!tu || !tv || !tw || !tp || !uf || !vf || !wf || !pf) throw AnbError(ANB_ERR_INVALID, "null BC array");
+    CK(cudaSetDevice(c->prm.device));
+    const int nB = c->nB, nI = c->nI;
+    std::vector<uint8_t> ty(nB);
+    std::vector<double> val((size_t)4 * nB);
+    bool pZero = true;
+    for (int b = 0; b < nB; ++b) {
+      const int patch = c->L.bPatch[b];
+      ty[b] = (uint8_t)((tu[patch] == 1 ? 1 : 0) | (tv[patch] == 1 ? 2 : 0) | (tw[patch] == 1 ? 4 : 0) |
+                        (tp[patch] == 1 ? 8 : 0));
+      val[b] = uf[nI + b];
+      val[(size_t)nB + b] = vf[nI + b];
+      val[(size_t)2 * nB + b] = wf[nI + b];
+      val[(size_t)3 * nB + b] = pf[nI + b];
+      if ((ty[b] & 8) && pf[nI + b] != 0.0) pZero = false;
+    }
+    CK(cudaMemcpy(c->dBType, ty.data(), nB, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->dBVal, val.data(), val.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->pZeroBC = pZero;
+    c->bcSet = true;
+    return ANB_OK;
+  });
+}
+
+int anb_set_state(anb_ctx* c, const double* u, const double* v, const double* w, const double* p) {
+  if (!c) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    if (!u || !v || !w || !p) throw AnbError(ANB_ERR_INVALID, "null state array");
+    CK(cudaSetDevice(c->prm.device));
+    const double* s3[3] = {u, v, w};
+    upload_cells(c, s3, c->U, 3);
+    const double* s1[1] = {p};
+    upload_cells(c, s1, c->P, 1);
+    CK(cudaMemset(c->phi, 0, sizeof(double) * ((size_t)c->nI + c->nB)));
+    c->stateSet = true;
+    return ANB_OK;
+  });
+}
+
+int anb_get_state(anb_ctx* c, double* u, double* v, double* w, double* p, double* phi) {
+  if (!c) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    CK(cudaSetDevice(c->prm.device));
+    double* d3[3] = {u, v, w};
+    download_cells(c, c->U, d3, 3);
+    double* d1[1] = {p};
+    if (p) download_cells(c, c->P, d1, 1);
+    if (phi) download_faces(c, c->phi, phi);
+    return ANB_OK;
+  });
+}
+
+int anb_simple_iterate(anb_ctx* c, int nsteps, double tolMass, double tolVel, anb_iter_stats* stats, int* done) {
+  if (!c) return ANB_ERR_INVALID;
+  if (done) *done = 0;
+  return guarded(c, [&]() -> int {
+    check_ready(c);
+    int status = ANB_OK;
+    for (int k = 0; k < nsteps; ++k) {
+      anb_iter_stats st{};
+      st.step = k + 1;
+      if (simple_step(c, &st) == ANB_NOT_CONVERGED) status = ANB_NOT_CONVERGED;
+      if (stats) stats[k] = st;
+      if (done) *done = k + 1;
+      if (!std::isfinite(st.mass_res) || st.mass_res > 1e50) {
+        c->err = "SIMPLE-like steady solve diverged.";
+        return ANB_ERR_DIVERGED;
+      }
+      if (st.mass_res < tolMass && std::max({st.du_rel, st.dv_rel, st.dw_rel}) < tolVel) break;
+    }
+    return status;
+  });
+}
+
+int anb_patch_force(anb_ctx* c, int patch, int sign, anb_force_report* out) {
+  if (!c || !out) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    std::memset(out, 0, sizeof(*out));
+    if (patch < 0 || patch >= (int)c->hm.patches.size()) return ANB_OK;  // valid = 0
+    CK(cudaSetDevice(c->prm.device));
+    const int b0 = c->hm.patches[patch].start - c->nI;
+    const int b1 = b0 + c->hm.patches[patch].nFaces;
+    launch_patch_force(c->stream, c->dm, b0, b1, sign, c->prm.mu, c->dBA, c->dBN, c->U, c->P, c->forceOut);
+    double h[16];
+    CK(cudaMemcpyAsync(h, c->forceOut, sizeof(double) * 15, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->valid = 1;
+    for (int k = 0; k < 3; ++k) {
+      out->Fp[k] = h[k];
+      out->Fv[k] = h[3 + k];
+      out->F[k] = h[6 + k];
+    }
+    out->area = h[9];
+    out->n_faces = (int)h[10];
+    out->min_wall_distance = h[11];
+    out->max_wall_distance = h[12];
+    out->max_ut = h[13];
+    out->max_shear_mag = h[14];
+    return ANB_OK;
+  });
+}
+
+int anb_debug_gradient(anb_ctx* c, int field, const double* phi, double* gx, double* gy, double* gz) {
+  if (!c) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    if (!c->bcSet) throw AnbError(ANB_ERR_INVALID, "boundary conditions not set");
+    if (field < 0 || field > 3) throw AnbError(ANB_ERR_INVALID, "field must be 0..3");
+    CK(cudaSetDevice(c->prm.device));
+    const double* s1[1] = {phi};
+    upload_cells(c, s1, c->pdx, 1);
+    const unsigned char bits[1] = {(unsigned char)(1u << field)};
+    const double* in[1] = {c->pdx};
+    double* outp[1] = {c->Gc};
+    grad(c, 1, in, bits, outp);
+    CK(cudaGetLastError());
+    double* d[3] = {gx, gy, gz};
+    download_cells(c, c->Gc, d, 3);
+    return ANB_OK;
+  });
+}
+
+int anb_debug_momentum(anb_ctx* c, const double* u, const double* v, const double* w, const double* p,
+                       double* diag, double* a_pn, double* a_np, double* rhs, double* rau) {
+  if (!c) return ANB_ERR_INVALID;
+  int rc = anb_set_state(c, u, v, w, p);
+  if (rc) return rc;
+  return guarded(c, [&]() -> int {
+    check_ready(c);
+    const int C = c->C;
+    const double* phi[4] = {c->U, c->U + C, c->U + 2 * C, c->P};
+    const unsigned char bits[4] = {1, 2, 4, 8};
+    double* out[4] = {c->G, c->G + 3 * C, c->G + 6 * C, c->G + 9 * C};
+    grad(c, 4, phi, bits, out);
+    MomArgs ma{};
+    ma.U = c->U;
+    ma.Q = c->U;
+    ma.G = c->G;
+    ma.rho = c->prm.rho;
+    ma.mu = c->prm.mu;
+    ma.uRelax = c->prm.u_relax;
+    ma.relax = c->prm.u_relax < 0.999999 ? 1 : 0;
+    ma.val = c->mval;
+    ma.diag = c->mdiag;
+    ma.rhs = c->rhs;
+    ma.rau = c->rau;
+    launch_momentum(c->lc, c->dm, ma);
+    CK(cudaGetLastError());
+    double* d1[1] = {diag};
+    if (diag) download_cells(c, c->mdiag, d1, 1);
+    double* r1[1] = {rau};
+    if (rau) download_cells(c, c->rau, r1, 1);
+    if (rhs) {
+      double* d3[3] = {rhs, rhs + C, rhs + 2 * C};
+      download_cells(c, c->rhs, d3, 3);
+    }
+    download_offdiag(c, c->mval, a_pn, a_np);
+    return ANB_OK;
+  });
+}
+
+int anb_debug_pressure(anb_ctx* c, const double* u, const double* v, const double* w, const double* p,
+                       const double* rau, double* diag, double* a_pn, double* phi_star, double* div_star) {
+  if (!c) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    if (!c->bcSet) throw AnbError(ANB_ERR_INVALID, "boundary conditions not set");
+    CK(cudaSetDevice(c->prm.device));
+    const int C = c->C;
+    const double* s3[3] = {u, v, w};
+    upload_cells(c, s3, c->Us, 3);
+    const double* s1[1] = {p};
+    upload_cells(c, s1, c->P, 1);
+    const double* s2[1] = {rau};
+    upload_cells(c, s2, c->rau, 1);
+    const double* phi[1] = {c->P};
+    const unsigned char bits[1] = {8};
+    double* out[1] = {c->G + 9 * C};
+    grad(c, 1, phi, bits, out);
+    PresArgs pa{};
+    pa.Us = c->Us;
+    pa.P = c->P;
+    pa.Gp = c->G + 9 * C;
+    pa.rau = c->rau;
+    pa.rho = c->prm.rho;
+    pa.val = c->pval;
+    pa.diag = c->pdiag;
+    pa.phiStar = c->phiStar;
+    pa.divStar = c->divStar;
+    pa.b = c->pb;
+    pa.pc = c->Pc;
+    launch_pressure_rc(c->lc, c->dm, pa);
+    CK(cudaGetLastError());
+    double* d1[1] = {diag};
+    if (diag) download_cells(c, c->pdiag, d1, 1);
+    double* d2[1] = {div_star};
+    if (div_star) download_cells(c, c->divStar, d2, 1);
+    if (a_pn) download_offdiag(c, c->pval, a_pn, nullptr);
+    if (phi_star) download_faces(c, c->phiStar, phi_star);
+    return ANB_OK;
+  });
+}
+
+int anb_debug_pressure_solve(anb_ctx* c, const double* b, double* x, int* iters, double* final_res) {
+  if (!c) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    CK(cudaSetDevice(c->prm.device));
+    const double* s1[1] = {b};
+    upload_cells(c, s1, c->pb, 1);
+    const double* s2[1] = {x};
+    upload_cells(c, s2, c->pdx, 1);
+    ensure_amg(c);
+    int its = 0;
+    bool cv = true;
+    solve_pressure(c, c->pb, c->pdx, c->prm.p_rel_tol, &its, &cv);
+    CK(cudaGetLastError());
+    double* d1[1] = {x};
+    download_cells(c, c->pdx, d1, 1);
+    double h[8];
+    CK(cudaMemcpy(h, c->scal + kScalPcg, sizeof(double) * 8, cudaMemcpyDeviceToHost));
+    if (iters) *iters = its;
+    if (final_res) *final_res = std::sqrt(h[4]);
+    return cv ? ANB_OK : ANB_NOT_CONVERGED;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// Device-side data structures shared by the SIMPLE kernels (sm_100a).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace anb {
+
+constexpr int kBlock = 256;
+constexpr int kWarp = 32;
+
+// One internal face, 64 bytes: two 32-byte sectors per gather.
+struct __align__(16) FaceRec {
+  double lam;     // clamped weight toward the neighbour (new orientation)
+  double g;       // A / max(n.d, 1e-30)
+  double t[3];    // S - g d  (non-orthogonal correction vector)
+  double d[3];    // cc_N - cc_P
+};
+
+// One boundary face, 80 bytes.
+struct __align__(16) BndRec {
+  double g;       // A / max(n.d_b, 1e-30)
+  double t[3];    // S - g d_b
+  double S[3];    // area vector (outward)
+  double d[3];    // x_f - cc_P
+};
+
+// Read-only mesh view passed by value to kernels.
+struct DMesh {
+  int nCells, nInternal, nBoundary, nSlices;
+  const int* sliceOff;
+  const int* col;
+  const int* slotFace;
+  const FaceRec* face;
+  const uint8_t* fFlags;
+  const int* bOwner;
+  const BndRec* bnd;
+  const uint8_t* bFlags;
+  const int* cbOff;
+  const int* cbList;
+  const double* vol;
+  const double* cc;     // 3 per cell
+  const double* minv;   // 6 per cell
+  // boundary conditions per boundary face: bit0 u, bit1 v, bit2 w, bit3 p Dirichlet
+  const uint8_t* bType;
+  const double* bVal;   // 4 * nBoundary: u | v | w | p face values
+};
+
+// Generic SELL-32 sparse matrix (off-diagonals) + separate diagonal.
+struct DSell {
+  int n;
+  const int* sliceOff;
+  const int* col;
+  const double* val;
+  const double* diag;
+};
+
+// Cross-block deterministic reductions: each block writes a partial, the last block to arrive
+// (atomic ticket) combines the partials in block order.
+struct Reducer {
+  double* partials;     // [maxBlocks * maxQ]
+  unsigned int* ticket; // one counter, returns to 0 after each use
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Reduces NQ per-thread values over the block; result valid in thread 0.  ops: bit q set -> max.
+template <int NQ>
+__device__ __forceinline__ void block_reduce(double (&v)[NQ], unsigned maxMask, double* smem /*NQ*32*/) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = ((maxMask >> q) & 1u) ? warp_max(v[q]) : warp_sum(v[q]);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) smem[q * 32 + wid] = v[q];
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double x = lane < nw ? smem[q * 32 + lane] : (((maxMask >> q) & 1u) ? -1.0e308 : 0.0);
+      v[q] = ((maxMask >> q) & 1u) ? warp_max(x) : warp_sum(x);
+    }
+  }
+  __syncthreads();
+}
+
+// Block partial -> global; returns true in every thread of the last block, whose thread 0 then
+// holds the grid-wide result in v.
+template <int NQ>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NQ], unsigned maxMask, Reducer red, double* smem) {
+  block_reduce<NQ>(v, maxMask, smem);
+  __shared__ bool isLast;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) red.partials[(size_t)blockIdx.x * NQ + q] = v[q];
+    __threadfence();
+    unsigned t = atomicAdd(red.ticket, 1u);
+    isLast = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!isLast) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) v[q] = ((maxMask >> q) & 1u) ? -1.0e308 : 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const double x = __ldcg(&red.partials[(size_t)b * NQ + q]);
+      v[q] = ((maxMask >> q) & 1u) ? fmax(v[q], x) : v[q] + x;
+    }
+  }
+  block_reduce<NQ>(v, maxMask, smem);
+  if (threadIdx.x == 0) *red.ticket = 0u;
+  return true;
+}
+
+}  // namespace anb

@@ -1,0 +1,770 @@
+// Host-side polyMesh reader/writer, geometry and synthetic channel meshes.
+// Reader grammar and geometry follow apps/generic_simple_v1/src/main.cu:532-599.
+#include "host_mesh.hpp"
+
+#include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <sys/stat.h>
+#include <tuple>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace anb {
+namespace {
+
+inline Vec3 add3(const Vec3& a, const Vec3& b) { return {a[0] + b[0], a[1] + b[1], a[2] + b[2]}; }
+inline Vec3 sub3(const Vec3& a, const Vec3& b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+inline Vec3 mul3(double s, const Vec3& a) { return {s * a[0], s * a[1], s * a[2]}; }
+inline double dot3(const Vec3& a, const Vec3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline Vec3 cross3(const Vec3& a, const Vec3& b) {
+  return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+inline double norm3(const Vec3& a) { return std::sqrt(dot3(a, a)); }
+
+std::string read_file(const std::string& fn) {
+  std::ifstream in(fn, std::ios::binary);
+  if (!in) throw std::runtime_error("Could not open " + fn);
+  std::string s;
+  in.seekg(0, std::ios::end);
+  std::streamoff n = in.tellg();
+  if (n > 0) {
+    s.resize((size_t)n);
+    in.seekg(0, std::ios::beg);
+    in.read(&s[0], n);
+  }
+  return s;
+}
+
+// Removes /* */ blocks (an unterminated one stays) and // line comments, main.cu:533-537.
+std::string strip_comments(const std::string& txt) {
+  std::string s;
+  s.reserve(txt.size());
+  size_t i = 0, n = txt.size();
+  bool blocks = true;
+  while (i < n) {
+    if (blocks && txt[i] == '/' && i + 1 < n && txt[i + 1] == '*') {
+      size_t e = txt.find("*/", i + 2);
+      if (e == std::string::npos) {
+        blocks = false;
+        continue;
+      }
+      i = e + 2;
+      continue;
+    }
+    s.push_back(txt[i]);
+    ++i;
+  }
+  std::string out;
+  out.reserve(s.size() + 1);
+  size_t a = 0;
+  while (a < s.size()) {
+    size_t e = s.find('\n', a);
+    size_t lineEnd = (e == std::string::npos) ? s.size() : e;
+    size_t c = s.find("//", a);
+    size_t cut = (c != std::string::npos && c < lineEnd) ? c : lineEnd;
+    out.append(s, a, cut - a);
+    out.push_back('\n');
+    if (e == std::string::npos) break;
+    a = e + 1;
+  }
+  return out;
+}
+
+// First "<digits> (" opens the top-level list; returns its inside (main.cu:538-546).
+std::pair<size_t, size_t> main_list_range(const std::string& t) {
+  size_t start = std::string::npos, open = std::string::npos;
+  for (size_t i = 0; i < t.size(); ++i) {
+    if (std::isdigit((unsigned char)t[i])) {
+      size_t j = i;
+      while (j < t.size() && std::isdigit((unsigned char)t[j])) ++j;
+      while (j < t.size() && std::isspace((unsigned char)t[j])) ++j;
+      if (j < t.size() && t[j] == '(') {
+        start = i;
+        open = j;
+        break;
+      }
+    }
+  }
+  if (start == std::string::npos) throw std::runtime_error("Could not locate top-level OpenFOAM list");
+  int depth = 0;
+  size_t close = std::string::npos;
+  for (size_t i = open; i < t.size(); ++i) {
+    if (t[i] == '(') ++depth;
+    else if (t[i] == ')') {
+      --depth;
+      if (depth == 0) {
+        close = i;
+        break;
+      }
+    }
+  }
+  if (close == std::string::npos) throw std::runtime_error("Failed to match parentheses");
+  return {open + 1, close};
+}
+
+// istream-like integer parse inside [p, e): skips whitespace, returns false if no integer.
+inline bool parse_int(const char*& p, const char* e, int& v) {
+  while (p < e && std::isspace((unsigned char)*p)) ++p;
+  const char* q = p;
+  bool neg = false;
+  if (q < e && (*q == '-' || *q == '+')) {
+    neg = (*q == '-');
+    ++q;
+  }
+  if (q >= e || !std::isdigit((unsigned char)*q)) return false;
+  long long acc = 0;
+  while (q < e && std::isdigit((unsigned char)*q)) {
+    acc = acc * 10 + (*q - '0');
+    ++q;
+  }
+  v = (int)(neg ? -acc : acc);
+  p = q;
+  return true;
+}
+
+inline bool parse_double(const char*& p, const char* e, double& v) {
+  while (p < e && std::isspace((unsigned char)*p)) ++p;
+  if (p >= e) return false;
+  char buf[64];
+  size_t len = 0;
+  while (p + len < e && len < 63 && !std::isspace((unsigned char)p[len]) && p[len] != ')') {
+    buf[len] = p[len];
+    ++len;
+  }
+  buf[len] = 0;
+  char* end = nullptr;
+  errno = 0;
+  double d = std::strtod(buf, &end);
+  if (end == buf) return false;
+  v = d;
+  p += (end - buf);
+  return true;
+}
+
+std::vector<Vec3> read_points(const std::string& fn) {
+  std::string t = strip_comments(read_file(fn));
+  auto r = main_list_range(t);
+  std::vector<Vec3> P;
+  const char* base = t.data();
+  size_t pos = r.first;
+  while (true) {
+    size_t a = t.find('(', pos);
+    if (a == std::string::npos || a >= r.second) break;
+    size_t b = t.find(')', a + 1);
+    if (b == std::string::npos || b > r.second) break;
+    const char* p = base + a + 1;
+    const char* e = base + b;
+    Vec3 x{0.0, 0.0, 0.0};
+    for (int k = 0; k < 3; ++k)
+      if (!parse_double(p, e, x[k])) break;
+    P.push_back(x);
+    pos = b + 1;
+  }
+  return P;
+}
+
+void read_faces(const std::string& fn, std::vector<int>& off, std::vector<int>& pts) {
+  std::string t = strip_comments(read_file(fn));
+  auto r = main_list_range(t);
+  off.assign(1, 0);
+  pts.clear();
+  const char* base = t.data();
+  size_t pos = r.first, end = r.second;
+  while (pos < end) {
+    while (pos < end && std::isspace((unsigned char)t[pos])) ++pos;
+    if (pos >= end) break;
+    if (!std::isdigit((unsigned char)t[pos])) {
+      ++pos;
+      continue;
+    }
+    size_t q = pos;
+    long long k = 0;
+    while (q < end && std::isdigit((unsigned char)t[q])) {
+      k = k * 10 + (t[q] - '0');
+      ++q;
+    }
+    while (q < end && std::isspace((unsigned char)t[q])) ++q;
+    if (q >= end || t[q] != '(') throw std::runtime_error("Malformed faces list");
+    size_t rr = t.find(')', q + 1);
+    if (rr == std::string::npos || rr > end) throw std::runtime_error("Malformed faces list");
+    const char* p = base + q + 1;
+    const char* e = base + rr;
+    bool ok = true;
+    for (long long i = 0; i < k; ++i) {
+      int v = 0;
+      if (ok && !parse_int(p, e, v)) {
+        ok = false;
+        v = 0;
+      }
+      pts.push_back(ok ? v : 0);
+    }
+    off.push_back((int)pts.size());
+    pos = rr + 1;
+  }
+}
+
+std::vector<int> read_labels(const std::string& fn) {
+  std::string t = strip_comments(read_file(fn));
+  auto r = main_list_range(t);
+  std::vector<int> v;
+  const char* p = t.data() + r.first;
+  const char* e = t.data() + r.second;
+  int x;
+  while (parse_int(p, e, x)) {
+    v.push_back(x);
+    if (p < e && !std::isspace((unsigned char)*p)) break;
+  }
+  return v;
+}
+
+std::vector<PatchInfo> read_boundary(const std::string& fn) {
+  std::string t = strip_comments(read_file(fn));
+  auto r = main_list_range(t);
+  std::string inside = t.substr(r.first, r.second - r.first);
+  std::vector<PatchInfo> out;
+  size_t pos = 0;
+  while (pos < inside.size()) {
+    while (pos < inside.size() && std::isspace((unsigned char)inside[pos])) ++pos;
+    if (pos >= inside.size()) break;
+    if (!(std::isalpha((unsigned char)inside[pos]) || inside[pos] == '_')) {
+      ++pos;
+      continue;
+    }
+    size_t a = pos;
+    while (pos < inside.size() && (std::isalnum((unsigned char)inside[pos]) || inside[pos] == '_')) ++pos;
+    std::string name = inside.substr(a, pos - a);
+    while (pos < inside.size() && std::isspace((unsigned char)inside[pos])) ++pos;
+    if (pos >= inside.size() || inside[pos] != '{') continue;
+    int depth = 1;
+    size_t bodyStart = ++pos;
+    while (pos < inside.size() && depth > 0) {
+      if (inside[pos] == '{') ++depth;
+      else if (inside[pos] == '}') --depth;
+      ++pos;
+    }
+    std::string body = inside.substr(bodyStart, pos - bodyStart - 1);
+    auto find_int = [&](const std::string& key) -> int {
+      size_t k = body.find(key);
+      if (k == std::string::npos) return 0;
+      k += key.size();
+      while (k < body.size() && !std::isdigit((unsigned char)body[k]) && body[k] != '-') ++k;
+      size_t e = k;
+      while (e < body.size() && (std::isdigit((unsigned char)body[e]) || body[e] == '-')) ++e;
+      return std::atoi(body.substr(k, e - k).c_str());
+    };
+    auto find_word = [&](const std::string& key) -> std::string {
+      size_t k = body.find(key);
+      if (k == std::string::npos) return "";
+      k += key.size();
+      while (k < body.size() && std::isspace((unsigned char)body[k])) ++k;
+      size_t e = k;
+      while (e < body.size() && (std::isalnum((unsigned char)body[e]) || body[e] == '_')) ++e;
+      return body.substr(k, e - k);
+    };
+    PatchInfo p;
+    p.name = name;
+    p.nFaces = find_int("nFaces");
+    p.start = find_int("startFace");
+    p.type = find_word("type");
+    out.push_back(p);
+  }
+  return out;
+}
+
+void write_header(std::ostream& o, const char* cls, const char* obj, const std::string& note) {
+  o << "/*--------------------------------*- C++ -*----------------------------------*\\\n"
+       "  Written by anabasis_b200 (synthetic mesh)\n"
+       "\\*---------------------------------------------------------------------------*/\n"
+       "FoamFile\n{\n    format      ascii;\n    class       "
+    << cls << ";\n";
+  if (!note.empty()) o << "    note        \"" << note << "\";\n";
+  o << "    location    \"constant/polyMesh\";\n    object      " << obj
+    << ";\n}\n// * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * //\n\n";
+}
+
+void mkdir_p(const std::string& dir) {
+  std::string cur;
+  for (size_t i = 0; i <= dir.size(); ++i) {
+    if (i == dir.size() || dir[i] == '/') {
+      if (!cur.empty()) ::mkdir(cur.c_str(), 0755);
+    }
+    if (i < dir.size()) cur.push_back(dir[i]);
+  }
+}
+
+}  // namespace
+
+void finalize_topology(HostMesh& m) {
+  m.nFaces = (int)m.faceOff.size() - 1;
+  m.nInternalFaces = (int)m.neigh.size();
+  if ((int)m.owner.size() < m.nFaces)
+    throw std::runtime_error("owner list shorter than faces list");
+  m.owner.resize(m.nFaces);
+  m.nCells = 0;
+  for (int v : m.owner) m.nCells = std::max(m.nCells, v + 1);
+  for (int v : m.neigh) m.nCells = std::max(m.nCells, v + 1);
+  m.bPatch.assign(m.nFaces, 0);
+  for (size_t k = 0; k < m.patches.size(); ++k)
+    for (int f = m.patches[k].start; f < m.patches[k].start + m.patches[k].nFaces; ++f)
+      if (f >= 0 && f < m.nFaces) m.bPatch[f] = (int)k + 1;
+  // cell -> faces: owned faces ascending, then neighbour faces ascending (main.cu:588-590)
+  std::vector<int> cnt(m.nCells + 1, 0);
+  for (int f = 0; f < m.nFaces; ++f) {
+    if (m.owner[f] < 0) throw std::runtime_error("negative owner label at face " + std::to_string(f));
+    cnt[m.owner[f] + 1]++;
+  }
+  for (int f = 0; f < m.nInternalFaces; ++f) {
+    if (m.neigh[f] < 0) throw std::runtime_error("negative neighbour label at face " + std::to_string(f));
+    cnt[m.neigh[f] + 1]++;
+  }
+  m.cellFaceOff.assign(m.nCells + 1, 0);
+  for (int c = 0; c < m.nCells; ++c) m.cellFaceOff[c + 1] = m.cellFaceOff[c] + cnt[c + 1];
+  m.cellFaces.assign(m.cellFaceOff[m.nCells], 0);
+  m.cellFaceOri.assign(m.cellFaceOff[m.nCells], 0);
+  std::vector<int> fill(m.cellFaceOff.begin(), m.cellFaceOff.end() - 1);
+  for (int f = 0; f < m.nFaces; ++f) {
+    int P = m.owner[f];
+    m.cellFaces[fill[P]] = f;
+    m.cellFaceOri[fill[P]++] = 1;
+  }
+  for (int f = 0; f < m.nInternalFaces; ++f) {
+    int N = m.neigh[f];
+    m.cellFaces[fill[N]] = f;
+    m.cellFaceOri[fill[N]++] = -1;
+  }
+}
+
+// main.cu:591-597, same operation order.
+void compute_geometry(HostMesh& m, int nThreads) {
+#ifdef _OPENMP
+  if (nThreads > 0) omp_set_num_threads(nThreads);
+#else
+  (void)nThreads;
+#endif
+  const int nC = m.nCells, nF = m.nFaces;
+  for (int f = 0; f < nF; ++f)
+    for (int k = m.faceOff[f]; k < m.faceOff[f + 1]; ++k)
+      if (m.facePts[k] < 0 || m.facePts[k] >= m.nPoints())
+        throw std::runtime_error("face " + std::to_string(f) + " references a missing point");
+  m.cc.assign(nC, {0, 0, 0});
+  m.vol.assign(nC, 0.0);
+  int badCell = -1;
+#pragma omp parallel
+  {
+    std::vector<int> verts;
+    std::vector<int> fv;
+#pragma omp for schedule(static)
+    for (int c = 0; c < nC; ++c) {
+      verts.clear();
+      for (int j = m.cellFaceOff[c]; j < m.cellFaceOff[c + 1]; ++j) {
+        int f = m.cellFaces[j];
+        for (int k = m.faceOff[f]; k < m.faceOff[f + 1]; ++k) verts.push_back(m.facePts[k]);
+      }
+      std::sort(verts.begin(), verts.end());
+      verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
+      Vec3 c0{0, 0, 0};
+      for (int v : verts) c0 = add3(c0, m.points[v]);
+      c0 = mul3(1.0 / std::max((int)verts.size(), 1), c0);
+      double V = 0.0;
+      Vec3 M{0, 0, 0};
+      for (int j = m.cellFaceOff[c]; j < m.cellFaceOff[c + 1]; ++j) {
+        int f = m.cellFaces[j];
+        fv.assign(m.facePts.begin() + m.faceOff[f], m.facePts.begin() + m.faceOff[f + 1]);
+        if (m.cellFaceOri[j] < 0) std::reverse(fv.begin(), fv.end());
+        const Vec3 a = m.points[fv[0]];
+        for (size_t i = 1; i + 1 < fv.size(); ++i) {
+          const Vec3 b = m.points[fv[i]], d = m.points[fv[i + 1]];
+          double vTet = dot3(sub3(a, c0), cross3(sub3(b, c0), sub3(d, c0))) / 6.0;
+          Vec3 cTet = mul3(0.25, add3(add3(c0, a), add3(b, d)));
+          V += vTet;
+          M = add3(M, mul3(vTet, cTet));
+        }
+      }
+      if (V <= 0) {
+#pragma omp critical
+        if (badCell < 0 || c < badCell) badCell = c;
+      } else {
+        m.vol[c] = V;
+        m.cc[c] = mul3(1.0 / V, M);
+      }
+    }
+  }
+  if (badCell >= 0) throw std::runtime_error("Non-positive cell volume at cell " + std::to_string(badCell));
+  m.xf.assign(nF, {0, 0, 0});
+  m.Af.assign(nF, 0.0);
+  m.nf.assign(nF, {0, 0, 0});
+  m.Sf.assign(nF, {0, 0, 0});
+  int badFace = -1;
+#pragma omp parallel for schedule(static)
+  for (int f = 0; f < nF; ++f) {
+    const int b0 = m.faceOff[f], nv = m.faceOff[f + 1] - b0;
+    Vec3 xfc{0, 0, 0};
+    for (int k = 0; k < nv; ++k) xfc = add3(xfc, m.points[m.facePts[b0 + k]]);
+    xfc = mul3(1.0 / std::max(nv, 1), xfc);
+    m.xf[f] = xfc;
+    const Vec3 a = m.points[m.facePts[b0]];
+    Vec3 areaVec{0, 0, 0};
+    for (int i = 1; i + 1 < nv; ++i) {
+      const Vec3 b = m.points[m.facePts[b0 + i]], d = m.points[m.facePts[b0 + i + 1]];
+      areaVec = add3(areaVec, mul3(0.5, cross3(sub3(b, a), sub3(d, a))));
+    }
+    double areaMag = norm3(areaVec);
+    if (areaMag <= 1e-30) {
+#pragma omp critical
+      if (badFace < 0 || f < badFace) badFace = f;
+      continue;
+    }
+    Vec3 nloc = mul3(1.0 / areaMag, areaVec);
+    const int P = m.owner[f];
+    Vec3 dtest = (f < m.nInternalFaces) ? sub3(m.cc[m.neigh[f]], m.cc[P]) : sub3(m.xf[f], m.cc[P]);
+    if (dot3(nloc, dtest) < 0) nloc = mul3(-1.0, nloc);
+    m.Af[f] = areaMag;
+    m.nf[f] = nloc;
+    m.Sf[f] = mul3(areaMag, nloc);
+  }
+  if (badFace >= 0) throw std::runtime_error("Degenerate face area at face " + std::to_string(badFace));
+  double mx = 0.0;
+#pragma omp parallel for reduction(max : mx) schedule(static)
+  for (int f = 0; f < m.nInternalFaces; ++f) {
+    Vec3 d = sub3(m.cc[m.neigh[f]], m.cc[m.owner[f]]);
+    double cosang = std::fabs(dot3(d, m.nf[f])) / std::max(norm3(d), 1e-30);
+    cosang = std::min(1.0, std::max(0.0, cosang));
+    mx = std::max(mx, std::acos(cosang) * 180.0 / M_PI);
+  }
+  m.maxNonOrthDeg = mx;
+}
+
+HostMesh read_polymesh(const std::string& dir) {
+  HostMesh m;
+  m.patches = read_boundary(dir + "/boundary");
+  m.points = read_points(dir + "/points");
+  read_faces(dir + "/faces", m.faceOff, m.facePts);
+  m.owner = read_labels(dir + "/owner");
+  m.neigh = read_labels(dir + "/neighbour");
+  finalize_topology(m);
+  compute_geometry(m);
+  return m;
+}
+
+void write_polymesh(const HostMesh& m, const std::string& dir) {
+  mkdir_p(dir);
+  const int nF = (int)m.faceOff.size() - 1;
+  std::string note = "nPoints:" + std::to_string(m.points.size()) + "  nCells:" + std::to_string(m.nCells) +
+                     "  nFaces:" + std::to_string(nF) + "  nInternalFaces:" + std::to_string(m.neigh.size());
+  {
+    std::FILE* fp = std::fopen((dir + "/points").c_str(), "w");
+    if (!fp) throw std::runtime_error("Could not open " + dir + "/points for writing");
+    std::ostringstream h;
+    write_header(h, "vectorField", "points", "");
+    std::fputs(h.str().c_str(), fp);
+    std::fprintf(fp, "%zu\n(\n", m.points.size());
+    for (const auto& p : m.points) std::fprintf(fp, "(%.17g %.17g %.17g)\n", p[0], p[1], p[2]);
+    std::fputs(")\n", fp);
+    std::fclose(fp);
+  }
+  {
+    std::FILE* fp = std::fopen((dir + "/faces").c_str(), "w");
+    if (!fp) throw std::runtime_error("Could not open " + dir + "/faces for writing");
+    std::ostringstream h;
+    write_header(h, "faceList", "faces", "");
+    std::fputs(h.str().c_str(), fp);
+    std::fprintf(fp, "%d\n(\n", nF);
+    for (int f = 0; f < nF; ++f) {
+      std::fprintf(fp, "%d(", m.faceOff[f + 1] - m.faceOff[f]);
+      for (int k = m.faceOff[f]; k < m.faceOff[f + 1]; ++k)
+        std::fprintf(fp, k + 1 < m.faceOff[f + 1] ? "%d " : "%d", m.facePts[k]);
+      std::fputs(")\n", fp);
+    }
+    std::fputs(")\n", fp);
+    std::fclose(fp);
+  }
+  auto write_labels = [&](const char* obj, const std::vector<int>& v, size_t n) {
+    std::FILE* fp = std::fopen((dir + "/" + obj).c_str(), "w");
+    if (!fp) throw std::runtime_error(std::string("Could not open ") + dir + "/" + obj + " for writing");
+    std::ostringstream h;
+    write_header(h, "labelList", obj, note);
+    std::fputs(h.str().c_str(), fp);
+    std::fprintf(fp, "%zu\n(\n", n);
+    for (size_t i = 0; i < n; ++i) std::fprintf(fp, "%d\n", v[i]);
+    std::fputs(")\n", fp);
+    std::fclose(fp);
+  };
+  write_labels("owner", m.owner, (size_t)nF);
+  write_labels("neighbour", m.neigh, m.neigh.size());
+  {
+    std::ofstream o(dir + "/boundary");
+    if (!o) throw std::runtime_error("Could not open " + dir + "/boundary for writing");
+    write_header(o, "polyBoundaryMesh", "boundary", "");
+    o << m.patches.size() << "\n(\n";
+    for (const auto& p : m.patches) {
+      o << "    " << p.name << "\n    {\n        type            " << (p.type.empty() ? "patch" : p.type)
+        << ";\n        physicalType    patch;\n        nFaces          " << p.nFaces
+        << ";\n        startFace       " << p.start << ";\n    }\n";
+    }
+    o << ")\n";
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Synthetic channel meshes
+// ---------------------------------------------------------------------------------------
+namespace {
+
+struct RawFace {
+  int owner, neigh, patch;  // neigh = -1 for boundary; patch index for boundary faces
+  int v[4];
+  int nv;
+};
+
+void assemble_faces(HostMesh& m, std::vector<RawFace>& faces, int nPatches, const char* const* names) {
+  std::vector<RawFace> internal, bnd;
+  for (auto& f : faces) (f.neigh >= 0 ? internal : bnd).push_back(f);
+  std::sort(internal.begin(), internal.end(), [](const RawFace& a, const RawFace& b) {
+    return a.owner != b.owner ? a.owner < b.owner : a.neigh < b.neigh;
+  });
+  std::stable_sort(bnd.begin(), bnd.end(), [](const RawFace& a, const RawFace& b) {
+    return a.patch != b.patch ? a.patch < b.patch : a.owner < b.owner;
+  });
+  m.faceOff.assign(1, 0);
+  m.facePts.clear();
+  m.owner.clear();
+  m.neigh.clear();
+  for (auto& f : internal) {
+    for (int k = 0; k < f.nv; ++k) m.facePts.push_back(f.v[k]);
+    m.faceOff.push_back((int)m.facePts.size());
+    m.owner.push_back(f.owner);
+    m.neigh.push_back(f.neigh);
+  }
+  m.patches.assign(nPatches, PatchInfo{});
+  for (int p = 0; p < nPatches; ++p) {
+    m.patches[p].name = names[p];
+    m.patches[p].type = "patch";
+  }
+  int cursor = (int)internal.size();
+  for (int p = 0; p < nPatches; ++p) m.patches[p].start = cursor;
+  for (auto& f : bnd) {
+    for (int k = 0; k < f.nv; ++k) m.facePts.push_back(f.v[k]);
+    m.faceOff.push_back((int)m.facePts.size());
+    m.owner.push_back(f.owner);
+    m.patches[f.patch].nFaces++;
+  }
+  for (int p = 0; p < nPatches; ++p) {
+    m.patches[p].start = cursor;
+    cursor += m.patches[p].nFaces;
+  }
+}
+
+}  // namespace
+
+HostMesh make_channel_mesh(const ChannelSpec& s) {
+  const int nx = s.nx, ny = s.ny, nz = s.nz;
+  if (nx < 1 || ny < 1 || nz < 1) throw std::runtime_error("channel mesh needs nx, ny, nz >= 1");
+  const double dx = s.Lx / nx, dy = s.Ly / ny, dz = s.Lz / nz;
+  auto nodeId = [&](int i, int j, int k) { return (k * (ny + 1) + j) * (nx + 1) + i; };
+  // obstacle cell-index box from unjittered cell centres
+  int i0 = 0, i1 = 0, j0 = 0, j1 = 0;
+  if (s.obstacle) {
+    i0 = nx; i1 = -1; j0 = ny; j1 = -1;
+    for (int i = 0; i < nx; ++i) {
+      double xc = (i + 0.5) * dx;
+      if (xc >= s.ox0 && xc <= s.ox1) { i0 = std::min(i0, i); i1 = std::max(i1, i + 1); }
+    }
+    for (int j = 0; j < ny; ++j) {
+      double yc = (j + 0.5) * dy;
+      if (yc >= s.oy0 && yc <= s.oy1) { j0 = std::min(j0, j); j1 = std::max(j1, j + 1); }
+    }
+    if (i1 <= i0 || j1 <= j0) throw std::runtime_error("obstacle block contains no cell centre");
+  }
+  auto solid = [&](int i, int j, int) {
+    return s.obstacle && i >= i0 && i < i1 && j >= j0 && j < j1;
+  };
+  // node coordinates with jitter; boundary nodes move only tangentially
+  const int nN = (nx + 1) * (ny + 1) * (nz + 1);
+  std::vector<Vec3> X(nN);
+  std::mt19937_64 rng(s.seed);
+  std::uniform_real_distribution<double> U(-1.0, 1.0);
+  for (int k = 0; k <= nz; ++k)
+    for (int j = 0; j <= ny; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        double rx = U(rng), ry = U(rng), rz = U(rng);
+        bool fixX = (i == 0 || i == nx), fixY = (j == 0 || j == ny), fixZ = (k == 0 || k == nz);
+        if (s.obstacle) {
+          bool onXFace = (i == i0 || i == i1) && j >= j0 && j <= j1;
+          bool onYFace = (j == j0 || j == j1) && i >= i0 && i <= i1;
+          fixX = fixX || onXFace;
+          fixY = fixY || onYFace;
+        }
+        Vec3 p{i * dx, j * dy, k * dz};
+        if (i == nx) p[0] = s.Lx;
+        if (j == ny) p[1] = s.Ly;
+        if (k == nz) p[2] = s.Lz;
+        if (s.jitter > 0.0) {
+          if (!fixX) p[0] += s.jitter * dx * rx;
+          if (!fixY) p[1] += s.jitter * dy * ry;
+          if (!fixZ) p[2] += s.jitter * dz * rz;
+        }
+        X[nodeId(i, j, k)] = p;
+      }
+  // hex cell ids
+  std::vector<int> hexId((size_t)nx * ny * nz, -1);
+  int nHex = 0;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        if (!solid(i, j, k)) hexId[((size_t)k * ny + j) * nx + i] = nHex++;
+  auto hid = [&](int i, int j, int k) -> int {
+    if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz) return -2;  // outside box
+    return hexId[((size_t)k * ny + j) * nx + i];                             // -1 = solid
+  };
+  const char* names[4] = {"patch_0_0", "patch_1_0", "patch_2_0", "patch_3_0"};
+  const int nPatches = s.obstacle ? 4 : 3;
+  HostMesh m;
+  std::vector<RawFace> faces;
+
+  if (!s.tets) {
+    faces.reserve((size_t)nHex * 3 + 2 * ((size_t)nx * ny + (size_t)ny * nz + (size_t)nx * nz));
+    // quad with +axis normal at node plane; a = cell on the low side, b = cell on the high side
+    auto quad = [&](int axis, int i, int j, int k, int v[4]) {
+      if (axis == 0) { v[0] = nodeId(i, j, k); v[1] = nodeId(i, j + 1, k); v[2] = nodeId(i, j + 1, k + 1); v[3] = nodeId(i, j, k + 1); }
+      else if (axis == 1) { v[0] = nodeId(i, j, k); v[1] = nodeId(i, j, k + 1); v[2] = nodeId(i + 1, j, k + 1); v[3] = nodeId(i + 1, j, k); }
+      else { v[0] = nodeId(i, j, k); v[1] = nodeId(i + 1, j, k); v[2] = nodeId(i + 1, j + 1, k); v[3] = nodeId(i, j + 1, k); }
+    };
+    for (int axis = 0; axis < 3; ++axis) {
+      const int ni = nx + (axis == 0), nj = ny + (axis == 1), nk = nz + (axis == 2);
+      for (int k = 0; k < nk; ++k)
+        for (int j = 0; j < nj; ++j)
+          for (int i = 0; i < ni; ++i) {
+            int lo = hid(i - (axis == 0), j - (axis == 1), k - (axis == 2));
+            int hi = hid(i, j, k);
+            RawFace f;
+            f.nv = 4;
+            quad(axis, i, j, k, f.v);
+            if (lo >= 0 && hi >= 0) {
+              f.owner = lo; f.neigh = hi; f.patch = -1;
+              faces.push_back(f);
+            } else if (lo >= 0 || hi >= 0) {
+              int patch;
+              bool outsideBox = (lo == -2 || hi == -2);
+              if (!outsideBox) patch = 3;
+              else if (axis == 0) patch = (lo == -2) ? 1 : 2;
+              else patch = 0;
+              f.neigh = -1; f.patch = patch;
+              if (lo >= 0) {
+                f.owner = lo;  // outward = +axis, keep order
+              } else {
+                f.owner = hi;  // outward = -axis, reverse
+                std::reverse(f.v, f.v + 4);
+              }
+              faces.push_back(f);
+            }
+          }
+    }
+    m.nCells = nHex;
+  } else {
+    // Kuhn split: tet = path 000 -> e_a -> e_a+e_b -> 111 over the 6 axis permutations.
+    static const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    struct TriKey { int a, b, c; int cell; int lf; };
+    std::vector<std::array<int, 4>> tetV;
+    tetV.reserve((size_t)nHex * 6);
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          if (hid(i, j, k) < 0) continue;
+          for (int p = 0; p < 6; ++p) {
+            int c[3] = {0, 0, 0};
+            std::array<int, 4> tv;
+            tv[0] = nodeId(i, j, k);
+            for (int s2 = 0; s2 < 3; ++s2) {
+              c[perms[p][s2]] = 1;
+              tv[s2 + 1] = nodeId(i + c[0], j + c[1], k + c[2]);
+            }
+            tetV.push_back(tv);
+          }
+        }
+    const int nTet = (int)tetV.size();
+    std::vector<TriKey> keys((size_t)nTet * 4);
+    static const int opp[4][3] = {{1, 2, 3}, {0, 2, 3}, {0, 1, 3}, {0, 1, 2}};
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < nTet; ++t)
+      for (int lf = 0; lf < 4; ++lf) {
+        int a = tetV[t][opp[lf][0]], b = tetV[t][opp[lf][1]], c = tetV[t][opp[lf][2]];
+        if (a > b) std::swap(a, b);
+        if (b > c) std::swap(b, c);
+        if (a > b) std::swap(a, b);
+        keys[(size_t)t * 4 + lf] = {a, b, c, t, lf};
+      }
+    std::sort(keys.begin(), keys.end(), [](const TriKey& x, const TriKey& y) {
+      if (x.a != y.a) return x.a < y.a;
+      if (x.b != y.b) return x.b < y.b;
+      if (x.c != y.c) return x.c < y.c;
+      return x.cell < y.cell;
+    });
+    auto centroid = [&](int t) {
+      Vec3 c{0, 0, 0};
+      for (int q = 0; q < 4; ++q) c = add3(c, X[tetV[t][q]]);
+      return mul3(0.25, c);
+    };
+    auto orient = [&](RawFace& f, int ownerTet) {
+      Vec3 a = X[f.v[0]], b = X[f.v[1]], c = X[f.v[2]];
+      Vec3 n = cross3(sub3(b, a), sub3(c, a));
+      Vec3 fc = mul3(1.0 / 3.0, add3(add3(a, b), c));
+      if (dot3(n, sub3(fc, centroid(ownerTet))) < 0) std::swap(f.v[1], f.v[2]);
+    };
+    auto nodeIJK = [&](int id, int& i, int& j, int& k) {
+      i = id % (nx + 1);
+      j = (id / (nx + 1)) % (ny + 1);
+      k = id / ((nx + 1) * (ny + 1));
+    };
+    faces.reserve((size_t)nTet * 2 + 1024);
+    for (size_t q = 0; q < keys.size();) {
+      RawFace f;
+      f.nv = 3;
+      f.v[0] = keys[q].a; f.v[1] = keys[q].b; f.v[2] = keys[q].c; f.v[3] = -1;
+      if (q + 1 < keys.size() && keys[q + 1].a == keys[q].a && keys[q + 1].b == keys[q].b &&
+          keys[q + 1].c == keys[q].c) {
+        f.owner = keys[q].cell; f.neigh = keys[q + 1].cell; f.patch = -1;
+        orient(f, f.owner);
+        faces.push_back(f);
+        q += 2;
+      } else {
+        f.owner = keys[q].cell; f.neigh = -1;
+        int ii[3], jj[3], kk[3];
+        for (int r = 0; r < 3; ++r) nodeIJK(f.v[r], ii[r], jj[r], kk[r]);
+        auto all = [&](const int* v, int val) { return v[0] == val && v[1] == val && v[2] == val; };
+        if (all(ii, 0)) f.patch = 1;
+        else if (all(ii, nx)) f.patch = 2;
+        else if (all(jj, 0) || all(jj, ny) || all(kk, 0) || all(kk, nz)) f.patch = 0;
+        else f.patch = 3;
+        orient(f, f.owner);
+        faces.push_back(f);
+        q += 1;
+      }
+    }
+    m.nCells = nTet;
+  }
+  assemble_faces(m, faces, nPatches, names);
+  // drop unused points (those inside the removed obstacle)
+  std::vector<int> used(nN, -1);
+  for (int v : m.facePts) used[v] = 0;
+  int np = 0;
+  for (int v = 0; v < nN; ++v)
+    if (used[v] == 0) used[v] = np++;
+  m.points.resize(np);
+  for (int v = 0; v < nN; ++v)
+    if (used[v] >= 0) m.points[used[v]] = X[v];
+  for (int& v : m.facePts) v = used[v];
+  finalize_topology(m);
+  return m;
+}
+
+}  // namespace anb

@@ -1,0 +1,17 @@
+// ASCII VTU writer of cell data on polyhedral cells (reference main.cu:975-983).
+#pragma once
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "host_mesh.hpp"
+
+namespace anb {
+
+// Writes points, polyhedron cells (type 42) and cell data: the vector field `vecName`
+// (vec[0..2], may be NULL) followed by the scalar fields.
+void write_vtu(const HostMesh& m, const std::string& filename, const std::vector<std::string>& names,
+               const std::vector<const double*>& data, const char* vecName, const double* const* vec);
+
+}  // namespace anb

@@ -1,0 +1,450 @@
+// Finite-volume face/cell kernels of the SIMPLE outer iteration (sm_100a).
+//
+// Every kernel is cell-centric over the SELL-32 layout: thread r owns row r, walks its
+// off-diagonal slots (one per neighbour, each slot naming the connecting face) and its boundary
+// faces, and accumulates diagonal, right-hand side and divergence in registers.  Each row writes
+// only its own outputs, so the reference's FP64 atomicAdd scatters (main.cu:56-58) become
+// deterministic gathers; a face's flux is written by its owner row.
+#include "kernels.cuh"
+
+namespace anb {
+
+namespace {
+
+__device__ __forceinline__ int row_base(const DMesh& m, int r, int& width) {
+  const int s = r >> 5;
+  const int b = __ldg(&m.sliceOff[s]);
+  width = (__ldg(&m.sliceOff[s + 1]) - b) >> 5;
+  return b + (r & 31);
+}
+
+__device__ __forceinline__ void load_face(const FaceRec* F, int f, double& lam, double& g, double t[3], double d[3]) {
+  const double2* p = reinterpret_cast<const double2*>(F + f);
+  const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), e = __ldg(p + 3);
+  lam = a.x; g = a.y; t[0] = b.x; t[1] = b.y; t[2] = c.x; d[0] = c.y; d[1] = e.x; d[2] = e.y;
+}
+
+__device__ __forceinline__ void load_bnd(const BndRec* B, int b, double& g, double t[3], double S[3], double d[3]) {
+  const double2* p = reinterpret_cast<const double2*>(B + b);
+  const double2 a = __ldg(p), c = __ldg(p + 1), e = __ldg(p + 2), h = __ldg(p + 3), k = __ldg(p + 4);
+  g = a.x; t[0] = a.y; t[1] = c.x; t[2] = c.y; S[0] = e.x; S[1] = e.y; S[2] = h.x; d[0] = h.y; d[1] = k.x; d[2] = k.y;
+}
+
+// ---- least-squares gradient: main.cu:1403-1440 on the moments of main.cu:1159-1251 ----------
+template <int NF>
+__global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
+  const int C = m.nCells;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
+    const double xr0 = m.cc[3 * r], xr1 = m.cc[3 * r + 1], xr2 = m.cc[3 * r + 2];
+    double pr[NF], b[NF][3];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      pr[f] = a.phi[f][r];
+      b[f][0] = b[f][1] = b[f][2] = 0.0;
+    }
+    int W;
+    const int base = row_base(m, r, W);
+    for (int k = 0; k < W; ++k) {
+      const int e = base + (k << 5);
+      if (__ldg(&m.slotFace[e]) < 0) break;
+      const int c = __ldg(&m.col[e]);
+      const double r0 = __ldg(&m.cc[3 * c]) - xr0, r1 = __ldg(&m.cc[3 * c + 1]) - xr1, r2 = __ldg(&m.cc[3 * c + 2]) - xr2;
+      const double w = 1.0 / fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-30);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        const double dp = w * (a.phi[f][c] - pr[f]);
+        b[f][0] += r0 * dp;
+        b[f][1] += r1 * dp;
+        b[f][2] += r2 * dp;
+      }
+    }
+    const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
+    for (int j = j0; j < j1; ++j) {
+      const int bf = __ldg(&m.cbList[j]);
+      const unsigned ty = __ldg(&m.bType[bf]);
+      const double* dd = m.bnd[bf].d;
+      const double r0 = dd[0], r1 = dd[1], r2 = dd[2];
+      const double w = 1.0 / fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-30);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        if (!(ty & a.bit[f])) continue;  // Neumann: phi_f = phi_P contributes nothing
+        const double dp = w * (a.bval[f][bf] - pr[f]);
+        b[f][0] += r0 * dp;
+        b[f][1] += r1 * dp;
+        b[f][2] += r2 * dp;
+      }
+    }
+    const double* M = m.minv + 6 * r;
+    const double m0 = M[0], m1 = M[1], m2 = M[2], m3 = M[3], m4 = M[4], m5 = M[5];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+      double* g = a.g[f];
+      g[r] = m0 * b[f][0] + m1 * b[f][1] + m2 * b[f][2];
+      g[C + r] = m1 * b[f][0] + m3 * b[f][1] + m4 * b[f][2];
+      g[2 * C + r] = m2 * b[f][0] + m4 * b[f][1] + m5 * b[f][2];
+    }
+  }
+}
+
+// ---- momentum: K25,K4,K2,K3,K5,K6 + rhs-only K26,K9,K7,K8,K10 for V and W in one pass ------
+// main.cu:1678-1896 (assembly), 1686-1695 (relaxation), 1787-1802 (rAU), loop 3350-3405.
+__global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgs a) {
+  const int C = m.nCells;
+  const double* U0 = a.U;
+  const double* U1 = a.U + C;
+  const double* U2 = a.U + 2 * C;
+  const bool full = !a.rhsOnly;
+  const double* G = a.G;
+  const double rho = a.rho, mu = a.mu;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
+    const double V = m.vol[r];
+    double rhs0 = -G[9 * C + r] * V, rhs1 = -G[10 * C + r] * V, rhs2 = -G[11 * C + r] * V;
+    double diag = 0.0;
+    const double ur0 = U0[r], ur1 = U1[r], ur2 = U2[r];
+    int W;
+    const int base = row_base(m, r, W);
+    for (int k = 0; k < W; ++k) {
+      const int e = base + (k << 5);
+      const int f = __ldg(&m.slotFace[e]);
+      if (f < 0) {
+        if (full) a.val[e] = 0.0;
+        continue;
+      }
+      if (!(__ldg(&m.fFlags[f]) & 1)) {
+        if (full) a.val[e] = 0.0;
+        continue;
+      }
+      const int c = __ldg(&m.col[e]);
+      const bool own = r < c;
+      double lam, g, t[3], d[3];
+      load_face(m.face, f, lam, g, t, d);
+      const int P = own ? r : c, N = own ? c : r;
+      const double l1 = 1.0 - lam;
+      const double alpha = mu * g;
+      const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
+      const double uc0 = l1 * U0[P] + lam * U0[N], uc1 = l1 * U1[P] + lam * U1[N], uc2 = l1 * U2[P] + lam * U2[N];
+      const double F = rho * (uc0 * S0 + uc1 * S1 + uc2 * S2);
+      double corr[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double* gq = G + 3 * q * C;
+        const double gx = l1 * gq[P] + lam * gq[N], gy = l1 * gq[C + P] + lam * gq[C + N],
+                     gz = l1 * gq[2 * C + P] + lam * gq[2 * C + N];
+        corr[q] = mu * (gx * t[0] + gy * t[1] + gz * t[2]);
+      }
+      if (own) {
+        if (full) a.val[e] = -alpha + F * lam;
+        diag += alpha + F * l1;
+        rhs0 += corr[0]; rhs1 += corr[1]; rhs2 += corr[2];
+      } else {
+        if (full) a.val[e] = -alpha - F * l1;
+        diag += alpha - F * lam;
+        rhs0 -= corr[0]; rhs1 -= corr[1]; rhs2 -= corr[2];
+      }
+    }
+    const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
+    for (int j = j0; j < j1; ++j) {
+      const int bf = __ldg(&m.cbList[j]);
+      if (!(__ldg(&m.bFlags[bf]) & 1)) continue;
+      double g, t[3], S[3], d[3];
+      load_bnd(m.bnd, bf, g, t, S, d);
+      const unsigned ty = __ldg(&m.bType[bf]);
+      const double alpha = mu * g;
+      const double bu = m.bVal[bf], bv = m.bVal[m.nBoundary + bf], bw = m.bVal[2 * m.nBoundary + bf];
+      const double ub = (ty & 1u) ? bu : ur0, vb = (ty & 2u) ? bv : ur1, wb = (ty & 4u) ? bw : ur2;
+      const double F = rho * (ub * S[0] + vb * S[1] + wb * S[2]);
+      diag += (ty & 1u) ? alpha : F;  // the matrix carries the u-component BC types
+      if (ty & 1u) rhs0 += alpha * bu + mu * (G[r] * t[0] + G[C + r] * t[1] + G[2 * C + r] * t[2]) - F * bu;
+      if (ty & 2u) rhs1 += alpha * bv + mu * (G[3 * C + r] * t[0] + G[4 * C + r] * t[1] + G[5 * C + r] * t[2]) - F * bv;
+      if (ty & 4u) rhs2 += alpha * bw + mu * (G[6 * C + r] * t[0] + G[7 * C + r] * t[1] + G[8 * C + r] * t[2]) - F * bw;
+    }
+    const double q0 = a.Q[r], q1 = a.Q[C + r], q2 = a.Q[2 * C + r];
+    if (full) {
+      if (a.relax) {
+        const double invR = 1.0 / a.uRelax;
+        const double aP = diag;
+        diag = aP * invR;
+        rhs0 += (invR - 1.0) * aP * q0;                 // K5 on the u pass
+        const double aPold = diag * a.uRelax;          // K10 on the v and w passes
+        rhs1 += (invR - 1.0) * aPold * q1;
+        rhs2 += (invR - 1.0) * aPold * q2;
+      }
+      a.diag[r] = diag;
+      a.rau[r] = fabs(diag) > 1e-30 ? V / diag : 0.0;
+    } else if (a.relax) {                                 // K10 for every re-solve
+      const double invR = 1.0 / a.uRelax;
+      const double aPold = a.diag[r] * a.uRelax;
+      rhs0 += (invR - 1.0) * aPold * q0;
+      rhs1 += (invR - 1.0) * aPold * q1;
+      rhs2 += (invR - 1.0) * aPold * q2;
+    }
+    a.rhs[r] = rhs0;
+    a.rhs[C + r] = rhs1;
+    a.rhs[2 * C + r] = rhs2;
+  }
+}
+
+// ---- pressure matrix (K11,K12) + Rhie-Chow flux (K14) + continuity (K15) ------------------
+// main.cu:1898-1950, 1474-1536, launch sequence 3407-3452.
+__global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgs a) {
+  const int C = m.nCells, nI = m.nInternal;
+  const double* U0 = a.Us;
+  const double* U1 = a.Us + C;
+  const double* U2 = a.Us + 2 * C;
+  const double* Gp = a.Gp;
+  const double rho = a.rho;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
+    double pd = 0.0, div = 0.0;
+    const double rAUr = a.rau[r];
+    int W;
+    const int base = row_base(m, r, W);
+    for (int k = 0; k < W; ++k) {
+      const int e = base + (k << 5);
+      const int f = __ldg(&m.slotFace[e]);
+      if (f < 0) {
+        a.val[e] = 0.0;
+        continue;
+      }
+      const int c = __ldg(&m.col[e]);
+      const bool own = r < c;
+      double lam, g, t[3], d[3];
+      load_face(m.face, f, lam, g, t, d);
+      const int P = own ? r : c, N = own ? c : r;
+      const double l1 = 1.0 - lam;
+      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
+      if (__ldg(&m.fFlags[f]) & 1) {
+        const double coeff = g * rAUf;
+        a.val[e] = -coeff;
+        pd += coeff;
+      } else {
+        a.val[e] = 0.0;
+      }
+      const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
+      const double ub = l1 * U0[P] + lam * U0[N], vb = l1 * U1[P] + lam * U1[N], wb = l1 * U2[P] + lam * U2[N];
+      const double gx = l1 * Gp[P] + lam * Gp[N], gy = l1 * Gp[C + P] + lam * Gp[C + N],
+                   gz = l1 * Gp[2 * C + P] + lam * Gp[2 * C + N];
+      const double phiI = rho * (ub * S0 + vb * S1 + wb * S2);
+      const double rc = rho * g * rAUf * ((a.P[N] - a.P[P]) - (gx * d[0] + gy * d[1] + gz * d[2]));
+      const double phi = phiI - rc;
+      if (own) {
+        div += phi;
+        a.phiStar[f] = phi;
+      } else {
+        div -= phi;
+      }
+    }
+    const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
+    for (int j = j0; j < j1; ++j) {
+      const int bf = __ldg(&m.cbList[j]);
+      double g, t[3], S[3], d[3];
+      load_bnd(m.bnd, bf, g, t, S, d);
+      const unsigned ty = __ldg(&m.bType[bf]);
+      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 1)) pd += g * rAUr;
+      const double uf = (ty & 1u) ? m.bVal[bf] : U0[r];
+      const double vf = (ty & 2u) ? m.bVal[m.nBoundary + bf] : U1[r];
+      const double wf = (ty & 4u) ? m.bVal[2 * m.nBoundary + bf] : U2[r];
+      const double phi = rho * (uf * S[0] + vf * S[1] + wf * S[2]);
+      div += phi;
+      a.phiStar[nI + bf] = phi;
+    }
+    a.diag[r] = pd;
+    a.divStar[r] = div;
+    a.b[r] = -div;
+    a.pc[r] = 0.0;
+  }
+}
+
+// ---- non-orthogonal divergence (K16) + pressure rhs (K17): main.cu:1538-1604 --------------
+__global__ void __launch_bounds__(kBlock) k_nonorth_rhs(DMesh m, NonOrthArgs a) {
+  const int C = m.nCells;
+  const double* Gc = a.Gc;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
+    double dno = 0.0;
+    int W;
+    const int base = row_base(m, r, W);
+    for (int k = 0; k < W; ++k) {
+      const int e = base + (k << 5);
+      const int f = __ldg(&m.slotFace[e]);
+      if (f < 0) break;
+      if (!(__ldg(&m.fFlags[f]) & 2)) continue;
+      const int c = __ldg(&m.col[e]);
+      const bool own = r < c;
+      double lam, g, t[3], d[3];
+      load_face(m.face, f, lam, g, t, d);
+      const int P = own ? r : c, N = own ? c : r;
+      const double l1 = 1.0 - lam;
+      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
+      const double gx = l1 * Gc[P] + lam * Gc[N], gy = l1 * Gc[C + P] + lam * Gc[C + N],
+                   gz = l1 * Gc[2 * C + P] + lam * Gc[2 * C + N];
+      const double flux = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
+      dno += own ? flux : -flux;
+    }
+    const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
+    for (int j = j0; j < j1; ++j) {
+      const int bf = __ldg(&m.cbList[j]);
+      if (!(__ldg(&m.bType[bf]) & 8u) || !(__ldg(&m.bFlags[bf]) & 2)) continue;
+      const double* t = m.bnd[bf].t;
+      dno += a.rau[r] * (Gc[r] * t[0] + Gc[C + r] * t[1] + Gc[2 * C + r] * t[2]);
+    }
+    a.b[r] = -a.divBase[r] + dno;
+  }
+}
+
+// ---- flux correction (K16 + K19) + continuity (K15) [+ K21, K20, step statistics] ----------
+// main.cu:1615-1658, 1523-1536, 3568-3603.
+__global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
+  __shared__ double sm[9 * 32];
+  const int C = m.nCells, nI = m.nInternal;
+  const double* Gc = a.Gc;
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
+    double div = 0.0;
+    const double pcr = a.pc[r], rAUr = a.rau[r];
+    int W;
+    const int base = row_base(m, r, W);
+    for (int k = 0; k < W; ++k) {
+      const int e = base + (k << 5);
+      const int f = __ldg(&m.slotFace[e]);
+      if (f < 0) break;
+      const int c = __ldg(&m.col[e]);
+      const bool own = r < c;
+      double lam, g, t[3], d[3];
+      load_face(m.face, f, lam, g, t, d);
+      const int P = own ? r : c, N = own ? c : r;
+      const double l1 = 1.0 - lam;
+      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
+      double phiNO = 0.0;
+      if (__ldg(&m.fFlags[f]) & 2) {
+        const double gx = l1 * Gc[P] + lam * Gc[N], gy = l1 * Gc[C + P] + lam * Gc[C + N],
+                     gz = l1 * Gc[2 * C + P] + lam * Gc[2 * C + N];
+        phiNO = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
+      }
+      const double phi = a.phiStar[f] - g * rAUf * (a.pc[N] - a.pc[P]) - phiNO;
+      if (own) {
+        div += phi;
+        a.phi[f] = phi;
+      } else {
+        div -= phi;
+      }
+    }
+    const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
+    for (int j = j0; j < j1; ++j) {
+      const int bf = __ldg(&m.cbList[j]);
+      const unsigned ty = __ldg(&m.bType[bf]);
+      double phi = a.phiStar[nI + bf];
+      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 2)) {
+        const double g = m.bnd[bf].g;
+        const double* t = m.bnd[bf].t;
+        const double phiNO = rAUr * (Gc[r] * t[0] + Gc[C + r] * t[1] + Gc[2 * C + r] * t[2]);
+        phi = phi - g * rAUr * (m.bVal[3 * m.nBoundary + bf] - pcr) - phiNO;
+      }
+      div += phi;
+      a.phi[nI + bf] = phi;
+    }
+    a.divCorr[r] = div;
+    if (a.update) {
+      const double pOld = a.P[r];
+      const double pNew = pOld + a.pRelax * pcr;
+      a.P[r] = pNew;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double uo = a.U[q * C + r];
+        const double un = a.Us[q * C + r] - rAUr * Gc[q * C + r];
+        a.U[q * C + r] = un;
+        const double dd = un - uo;
+        acc[2 * q] += dd * dd;
+        acc[2 * q + 1] += un * un;
+      }
+      const double dp = pNew - pOld;
+      acc[6] += dp * dp;
+      acc[7] += pNew * pNew;
+      acc[8] = fmax(acc[8], fabs(div));
+    }
+  }
+  if (!a.update) return;
+  if (grid_reduce<9>(acc, 1u << 8, a.red, sm) && threadIdx.x == 0)
+    for (int q = 0; q < 9; ++q) a.stats[q] = acc[q];
+}
+
+// ---- patch force: main.cu:2828-2933 (single block, deterministic order) -------------------
+__global__ void k_patch_force(DMesh m, int b0, int b1, int sign, double mu, const double* bA, const double* bN,
+                              const double* U, const double* P, double* out) {
+  __shared__ double sm[16 * 32];
+  const int C = m.nCells;
+  double v[16];
+  for (int q = 0; q < 16; ++q) v[q] = 0.0;
+  v[11] = -1.0e308;  // -min dn (as max)
+  v[12] = -1.0e308;  // max dn
+  v[13] = -1.0e308;  // max |Ut|
+  v[14] = -1.0e308;  // max shear
+  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
+    const int r = m.bOwner[b];
+    const double A = bA[b];
+    if (A <= 1.0e-300) continue;
+    double n0 = (double)sign * bN[3 * b], n1 = (double)sign * bN[3 * b + 1], n2 = (double)sign * bN[3 * b + 2];
+    const double nm = sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+    if (nm <= 1.0e-300) continue;
+    const double inv = 1.0 / nm;
+    n0 *= inv; n1 *= inv; n2 *= inv;
+    const double* d = m.bnd[b].d;  // x_f - cc_P
+    const double dx0 = -d[0], dx1 = -d[1], dx2 = -d[2];
+    double dn = dx0 * n0 + dx1 * n1 + dx2 * n2;
+    if (dn <= 1.0e-14) dn = fabs(dn);
+    if (dn <= 1.0e-14) dn = sqrt(dx0 * dx0 + dx1 * dx1 + dx2 * dx2);
+    if (dn <= 1.0e-14) continue;
+    const double u0 = U[r], u1 = U[C + r], u2 = U[2 * C + r];
+    const double Un = u0 * n0 + u1 * n1 + u2 * n2;
+    const double t0 = u0 - Un * n0, t1 = u1 - Un * n1, t2 = u2 - Un * n2;
+    const double Ut = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+    const double pr = P[r];
+    const double nn[3] = {n0, n1, n2}, tt[3] = {t0, t1, t2};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double fp = -pr * nn[q] * A, fv = mu * tt[q] / dn * A;
+      v[q] += fp;
+      v[3 + q] += fv;
+      v[6 + q] += fp + fv;
+    }
+    v[9] += A;
+    v[10] += 1.0;
+    v[11] = fmax(v[11], -dn);
+    v[12] = fmax(v[12], dn);
+    v[13] = fmax(v[13], Ut);
+    v[14] = fmax(v[14], mu * Ut / dn);
+  }
+  block_reduce<16>(v, (1u << 11) | (1u << 12) | (1u << 13) | (1u << 14), sm);
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 11; ++q) out[q] = v[q];
+    out[11] = v[10] > 0 ? -v[11] : 0.0;
+    out[12] = v[10] > 0 ? v[12] : 0.0;
+    out[13] = v[10] > 0 ? v[13] : 0.0;
+    out[14] = v[10] > 0 ? v[14] : 0.0;
+  }
+}
+
+}  // namespace
+
+void launch_lsq_grad(const LaunchCfg& lc, const DMesh& m, const GradArgs& a) {
+  if (a.nf == 4) k_lsq_grad<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (a.nf == 3) k_lsq_grad<3><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (a.nf == 2) k_lsq_grad<2><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else k_lsq_grad<1><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+}
+void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgs& a) {
+  k_momentum<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+}
+void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgs& a) {
+  k_pressure_rc<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+}
+void launch_nonorth_rhs(const LaunchCfg& lc, const DMesh& m, const NonOrthArgs& a) {
+  k_nonorth_rhs<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+}
+void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a) {
+  k_flux_final<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+}
+void launch_patch_force(cudaStream_t s, const DMesh& m, int b0, int b1, int sign, double mu, const double* bA,
+                        const double* bN, const double* U, const double* P, double* out) {
+  k_patch_force<<<1, 512, 0, s>>>(m, b0, b1, sign, mu, bA, bN, U, P, out);
+}
+
+}  // namespace anb

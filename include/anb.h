@@ -1,0 +1,159 @@
+/*
+ * anb.h - C ABI of the B200 SIMPLE library (libanb.so).
+ *
+ * The library replaces, for one GPU, everything the reference's generic_simple_v1 does between
+ * "mesh and boundary values are known" and "final fields are known": the 28 face/cell kernels
+ * of apps/generic_simple_v1/src/main.cu:1397-1967 and the HYPRE solves it drives
+ * (main.cu:1970-2676), orchestrated by the SIMPLE loop of main.cu:3350-3634.  The host program
+ * (reader, .case/.bc front end, VTU and summary writers) stays on the CPU side of this ABI.
+ *
+ * Conventions
+ *   - All arrays are host pointers owned by the caller; the library copies in on every call and
+ *     writes results into caller-allocated buffers.  The library owns all device memory and one
+ *     CUDA stream per context.
+ *   - All cell and face arrays use the caller's (OpenFOAM) numbering.  The library renumbers
+ *     internally (reverse Cuthill-McKee cells, owner-sorted faces) and maps back on output.
+ *   - Every function returns an ANB_* status.  ANB_NOT_CONVERGED is a warning (the reference's
+ *     HYPRE error 256: warn and continue); other non-zero values are errors whose text is
+ *     available from anb_last_error().  The library never calls exit() or abort().
+ *   - A context is not thread-safe; distinct contexts are independent.
+ */
+#ifndef ANB_H
+#define ANB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ANB_OK 0
+#define ANB_NOT_CONVERGED 1
+#define ANB_ERR_INVALID 2
+#define ANB_ERR_CUDA 3
+#define ANB_ERR_MESH 4
+#define ANB_ERR_IO 5
+#define ANB_ERR_UNSUPPORTED 6
+#define ANB_ERR_DIVERGED 7
+
+#define ANB_PRECISION_FP64 0
+#define ANB_PRECISION_MIXED 1
+
+typedef struct anb_ctx anb_ctx;
+
+/* polyMesh topology in OpenFOAM order (replaces the Mesh struct, main.cu:61-72). */
+typedef struct anb_mesh_desc {
+  int n_points;
+  const double* points;      /* 3*n_points, xyz interleaved */
+  int n_faces;
+  const int* face_offsets;   /* n_faces+1, CSR into face_points */
+  const int* face_points;
+  int n_internal_faces;
+  const int* owner;          /* n_faces */
+  const int* neighbour;      /* n_internal_faces */
+  int n_patches;
+  const int* patch_start;    /* n_patches */
+  const int* patch_size;     /* n_patches */
+} anb_mesh_desc;
+
+/* Solver controls; field meaning and defaults follow Params, main.cu:73-103. */
+typedef struct anb_params {
+  double rho, mu;
+  double u_relax, p_relax;
+  int n_nonorth_corr;        /* pressure non-orthogonal correctors (nNonOrthCorr)       */
+  int n_vel_nonorth_corr;    /* momentum re-solves (nVelNonOrthCorr)                     */
+  int n_pressure_corr;       /* extra pressure passes (nPressureCorr)                    */
+  int vel_maxit;
+  double vel_tol, vel_rel_tol;
+  int p_maxit;
+  double p_tol, p_rel_tol;
+  double corr_tol;
+  int p_amg_rebuild_every;   /* pressure preconditioner rebuild cadence (main.cu:3409)   */
+  int p_use_amg;             /* 1: aggregation-AMG preconditioned CG, 0: Jacobi CG       */
+  int precision;             /* ANB_PRECISION_FP64 or ANB_PRECISION_MIXED                */
+  int device;
+} anb_params;
+
+/* Per-outer-iteration monitor values (the stdout line of main.cu:3609-3611). */
+typedef struct anb_iter_stats {
+  int step;
+  int status;                /* ANB_OK or ANB_NOT_CONVERGED for this step's inner solves */
+  double mass_res, du_rel, dv_rel, dw_rel, dp_rel;
+  int its_u, its_v, its_w;   /* last BiCGSTAB iteration counts                            */
+  int its_p_last, its_p_total;
+  double iter_seconds;       /* device time of the step (CUDA events)                     */
+} anb_iter_stats;
+
+/* Force on a patch (compute_patch_forces_wall_shear, main.cu:2828-2933). */
+typedef struct anb_force_report {
+  int valid;
+  int n_faces;
+  double area;
+  double Fp[3], Fv[3], F[3];
+  double min_wall_distance, max_wall_distance, max_ut, max_shear_mag;
+} anb_force_report;
+
+/* Fills the reference defaults (main.cu:73-103). */
+void anb_default_params(anb_params* p);
+
+/* Builds the device layout: geometry (main.cu:582-599), RCM renumbering, face coefficients,
+ * least-squares gradient operator (main.cu:1159-1251), matrix patterns and the pressure AMG
+ * structure.  Replaces build_device_mesh / build_lsq_gradient_operator / init_*_system
+ * (main.cu:1072-1251, 2196-2273). */
+int anb_create(const anb_mesh_desc* mesh, const anb_params* params, anb_ctx** out);
+void anb_destroy(anb_ctx* ctx);
+const char* anb_last_error(const anb_ctx* ctx);
+
+/* Cell/face geometry in input numbering (any pointer may be NULL).  cc, xf, nf: 3 per entry. */
+int anb_get_geometry(anb_ctx* ctx, double* cc, double* vol, double* xf, double* nf, double* area,
+                     double* max_nonorth_deg);
+int anb_get_sizes(const anb_ctx* ctx, int* n_cells, int* n_faces, int* n_internal_faces, int* n_patches);
+
+/* Boundary conditions: per patch 1 = Dirichlet, 0 = Neumann (bc_to_int, main.cu:1058) and per
+ * face values (nFaces entries, internal entries ignored).  Replaces make_device_bc ×4
+ * (main.cu:1107-1114). */
+int anb_set_bc(anb_ctx* ctx, const int* type_u, const int* type_v, const int* type_w, const int* type_p,
+               const double* u_face, const double* v_face, const double* w_face, const double* p_face);
+
+/* Cell fields (u, v, w, p).  anb_set_state also resets the face flux to zero. */
+int anb_set_state(anb_ctx* ctx, const double* u, const double* v, const double* w, const double* p);
+int anb_get_state(anb_ctx* ctx, double* u, double* v, double* w, double* p, double* phi);
+
+/* Runs up to nsteps SIMPLE outer iterations (main.cu:3388-3634).  Stops early on
+ * convergence (massRes < tol_mass and max(du,dv,dw) < tol_vel) or divergence (massRes not
+ * finite or > 1e50, returns ANB_ERR_DIVERGED).  stats (may be NULL) receives one entry per
+ * executed step; *steps_done the count.  Returns ANB_NOT_CONVERGED if any inner solve hit
+ * its iteration cap. */
+int anb_simple_iterate(anb_ctx* ctx, int nsteps, double tol_mass, double tol_vel, anb_iter_stats* stats,
+                       int* steps_done);
+
+/* Pressure and wall-shear force integral over one patch on the device (main.cu:2828-2933);
+ * patch is the 0-based patch index in input order. */
+int anb_patch_force(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* out);
+
+/* ---- diagnostic entry points (parity tests of single stages) --------------------------------
+ * Each runs one stage of the outer iteration on the given host fields (input numbering) and
+ * returns its output in input numbering.  Internal-face coefficients are reported per face in
+ * the input orientation: a_pn = row owner / column neighbour, a_np = row neighbour / column
+ * owner.  Any output pointer may be NULL. */
+
+/* LSQ gradient of phi with the BC set of `field` (0 u, 1 v, 2 w, 3 p): kernel_apply_lsq_gradient,
+ * main.cu:1403-1440. */
+int anb_debug_gradient(anb_ctx* ctx, int field, const double* phi, double* gx, double* gy, double* gz);
+
+/* Momentum system for old fields (u,v,w,p): assembly + relaxation + rAU
+ * (main.cu:2346-2528).  rhs is 3*nCells (u, v, w components). */
+int anb_debug_momentum(anb_ctx* ctx, const double* u, const double* v, const double* w, const double* p,
+                       double* diag, double* a_pn, double* a_np, double* rhs, double* rau);
+
+/* Pressure matrix from rAU (main.cu:2532-2551) and the Rhie-Chow predicted flux + continuity
+ * (main.cu:1474-1536) for velocity (u,v,w) and pressure p. */
+int anb_debug_pressure(anb_ctx* ctx, const double* u, const double* v, const double* w, const double* p,
+                       const double* rau, double* diag, double* a_pn, double* phi_star, double* div_star);
+
+/* Solves the current pressure system A x = b with the configured preconditioned CG to
+ * (p_tol, p_rel_tol); x holds the initial guess on entry.  *iters receives the count. */
+int anb_debug_pressure_solve(anb_ctx* ctx, const double* b, double* x, int* iters, double* final_res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANB_H */

@@ -1,0 +1,155 @@
+"""CPU oracle of the SIMPLE outer iteration (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline/reference legs may import this
+package.  It wraps liboracle.so (oracle.cpp, a restatement of the reference's
+apps/generic_simple_v1/src/main.cu with file:line citations) and, when built, the reference's
+own host code compiled from the reference tree into oracle/_ref/ (see build.py).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_dp = ct.POINTER(ct.c_double)
+_ip = ct.POINTER(ct.c_int)
+_lib = None
+
+
+class OrcParams(ct.Structure):
+    _fields_ = [("rho", ct.c_double), ("mu", ct.c_double), ("u_relax", ct.c_double), ("p_relax", ct.c_double),
+                ("n_nonorth_corr", ct.c_int), ("n_vel_nonorth_corr", ct.c_int), ("n_pressure_corr", ct.c_int),
+                ("vel_maxit", ct.c_int), ("vel_tol", ct.c_double), ("vel_rel_tol", ct.c_double),
+                ("p_maxit", ct.c_int), ("p_tol", ct.c_double), ("p_rel_tol", ct.c_double),
+                ("corr_tol", ct.c_double), ("tol_mass", ct.c_double), ("tol_vel", ct.c_double),
+                ("n_threads", ct.c_int)]
+
+
+class OrcStats(ct.Structure):
+    _fields_ = [("mass_res", ct.c_double), ("du", ct.c_double), ("dv", ct.c_double), ("dw", ct.c_double),
+                ("dp", ct.c_double), ("its_u", ct.c_int), ("its_v", ct.c_int), ("its_w", ct.c_int),
+                ("its_p_last", ct.c_int), ("its_p_total", ct.c_int)]
+
+
+def lib() -> ct.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            from .build import build_oracle
+            build_oracle()
+        L = ct.CDLL(str(LIB))
+        L.orc_mesh_create.restype = ct.c_void_p
+        L.orc_mesh_create.argtypes = [ct.c_int, _dp, ct.c_int, _ip, _ip, ct.c_int, _ip, _ip, ct.c_int, _ip, _ip,
+                                      ct.c_char_p, ct.c_int]
+        L.orc_mesh_free.argtypes = [ct.c_void_p]
+        L.orc_mesh_ncells.restype = ct.c_int
+        L.orc_mesh_ncells.argtypes = [ct.c_void_p]
+        L.orc_mesh_geometry.argtypes = [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_set_bc.argtypes = [ct.c_void_p, _ip, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
+        L.orc_lsq_gradient.argtypes = [ct.c_void_p, ct.c_int, _dp, _dp, _dp, _dp]
+        L.orc_momentum.argtypes = [ct.c_void_p, ct.c_double, ct.c_double, ct.c_double, _dp, _dp, _dp, _dp, _dp, _dp,
+                                   _dp, _dp, _dp]
+        L.orc_pressure.argtypes = [ct.c_void_p, ct.c_double, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_simple_run.restype = ct.c_int
+        L.orc_simple_run.argtypes = [ct.c_void_p, ct.POINTER(OrcParams), ct.c_int, _dp, _dp, _dp, _dp, _dp,
+                                     ct.POINTER(OrcStats)]
+        L.orc_patch_force.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double, _dp, _dp, _dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return None if a is None else a.ctypes.data_as(_ip)
+
+
+class Oracle:
+    """Oracle mesh + boundary conditions; topology dict as returned by HostMesh.topology()."""
+
+    def __init__(self, topo: dict):
+        self.t = topo
+        nf = len(topo["face_offsets"]) - 1
+        err = ct.create_string_buffer(1024)
+        h = lib().orc_mesh_create(len(topo["points"]) // 3, _d(topo["points"]), nf, _i(topo["face_offsets"]),
+                                  _i(topo["face_points"]), len(topo["neighbour"]), _i(topo["owner"]),
+                                  _i(topo["neighbour"]), len(topo["patch_start"]), _i(topo["patch_start"]),
+                                  _i(topo["patch_size"]), err, 1024)
+        if not h:
+            raise RuntimeError(err.value.decode())
+        self._h = ct.c_void_p(h)
+        self.n_cells = lib().orc_mesh_ncells(self._h)
+        self.n_faces = nf
+        self.n_internal = len(topo["neighbour"])
+
+    def geometry(self) -> dict:
+        C, F = self.n_cells, self.n_faces
+        g = dict(cc=np.zeros(3 * C), vol=np.zeros(C), xf=np.zeros(3 * F), nf=np.zeros(3 * F), sf=np.zeros(3 * F),
+                 af=np.zeros(F))
+        mx = np.zeros(1)
+        lib().orc_mesh_geometry(self._h, _d(g["cc"]), _d(g["vol"]), _d(g["xf"]), _d(g["nf"]), _d(g["sf"]),
+                                _d(g["af"]), _d(mx))
+        g["max_nonorth"] = float(mx[0])
+        return g
+
+    def set_bc(self, bc: dict) -> None:
+        self._bc = bc
+        lib().orc_set_bc(self._h, _i(bc["type_u"]), _i(bc["type_v"]), _i(bc["type_w"]), _i(bc["type_p"]),
+                         _d(bc["u"]), _d(bc["v"]), _d(bc["w"]), _d(bc["p"]))
+
+    def gradient(self, field: int, phi) -> np.ndarray:
+        g = np.zeros((3, self.n_cells))
+        phi = np.ascontiguousarray(phi, np.float64)
+        lib().orc_lsq_gradient(self._h, field, _d(phi), _d(g[0]), _d(g[1]), _d(g[2]))
+        return g
+
+    def momentum(self, rho, mu, u_relax, u, v, w, p) -> dict:
+        C, I = self.n_cells, self.n_internal
+        o = dict(diag=np.zeros(C), a_pn=np.zeros(I), a_np=np.zeros(I), rhs=np.zeros(3 * C), rau=np.zeros(C))
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p)]
+        lib().orc_momentum(self._h, rho, mu, u_relax, *map(_d, arrs), _d(o["diag"]), _d(o["a_pn"]), _d(o["a_np"]),
+                           _d(o["rhs"]), _d(o["rau"]))
+        return o
+
+    def pressure(self, rho, u, v, w, p, rau) -> dict:
+        C, I, F = self.n_cells, self.n_internal, self.n_faces
+        o = dict(diag=np.zeros(C), a_pn=np.zeros(I), phi_star=np.zeros(F), div_star=np.zeros(C))
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p, rau)]
+        lib().orc_pressure(self._h, rho, *map(_d, arrs), _d(o["diag"]), _d(o["a_pn"]), _d(o["phi_star"]),
+                           _d(o["div_star"]))
+        return o
+
+    def run(self, params: OrcParams, nsteps: int, u, v, w, p) -> tuple[dict, list]:
+        st = (OrcStats * max(nsteps, 1))()
+        s = dict(u=np.array(u, np.float64), v=np.array(v, np.float64), w=np.array(w, np.float64),
+                 p=np.array(p, np.float64), phi=np.zeros(self.n_faces))
+        done = lib().orc_simple_run(self._h, ct.byref(params), nsteps, _d(s["u"]), _d(s["v"]), _d(s["w"]),
+                                    _d(s["p"]), _d(s["phi"]), st)
+        stats = [dict((f, getattr(st[i], f)) for f, _ in OrcStats._fields_) for i in range(done)]
+        return s, stats
+
+    def patch_force(self, patch, sign, mu, u, v, w, p) -> np.ndarray:
+        o = np.zeros(11)
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p)]
+        lib().orc_patch_force(self._h, patch, sign, mu, *map(_d, arrs), _d(o))
+        return o
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and _lib is not None:
+            _lib.orc_mesh_free(self._h)
+            self._h = None
+
+
+def params(**kw) -> OrcParams:
+    """Oracle controls with the reference defaults (main.cu:73-103)."""
+    p = OrcParams(rho=1.0, mu=0.05, u_relax=0.7, p_relax=1.0, n_nonorth_corr=2, n_vel_nonorth_corr=0,
+                  n_pressure_corr=0, vel_maxit=100, vel_tol=1e-10, vel_rel_tol=0.0, p_maxit=4000, p_tol=1e-10,
+                  p_rel_tol=0.0, corr_tol=1e-12, tol_mass=1e-10, tol_vel=1e-10, n_threads=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p

@@ -1,0 +1,81 @@
+/*
+ * oracle.h - CPU oracle for the SIMPLE outer iteration of the reference's generic_simple_v1.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the B200 library: only tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline / reference arm may load it.  The product
+ * (libanb.so and the anabasis_simple host program) never links or calls it.
+ *
+ * It restates, in plain serial/OpenMP C++, the reference's algorithm with each function citing
+ * the file:line it follows (apps/generic_simple_v1/src/main.cu, "GSV1" below).  Pinning status:
+ *   - geometry, LSQ gradient, Rhie-Chow, continuity, non-orthogonal flux, flux correction and
+ *     patch forces are checked against the reference's own host functions compiled from
+ *     /root/reference by oracle/build_ref.sh (tests/test_oracle_vs_reference.py);
+ *   - the linear solves of the reference are HYPRE 3.0.0 (not vendored, not installable here):
+ *     the oracle replaces them with deterministic FP64 Krylov solvers run to tight tolerance, so
+ *     solver-level parity is unpinned and parity is judged on converged/tightly-solved fields.
+ */
+#ifndef ANB_ORACLE_H
+#define ANB_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_mesh orc_mesh;
+
+typedef struct orc_params {
+  double rho, mu, u_relax, p_relax;
+  int n_nonorth_corr, n_vel_nonorth_corr, n_pressure_corr;
+  int vel_maxit; double vel_tol, vel_rel_tol;
+  int p_maxit; double p_tol, p_rel_tol;
+  double corr_tol, tol_mass, tol_vel;
+  int n_threads;
+} orc_params;
+
+typedef struct orc_stats {
+  double mass_res, du, dv, dw, dp;
+  int its_u, its_v, its_w, its_p_last, its_p_total;
+} orc_stats;
+
+/* topology in OpenFOAM order; returns NULL and fills err on failure */
+orc_mesh* orc_mesh_create(int n_points, const double* points, int n_faces, const int* face_off,
+                          const int* face_pts, int n_internal, const int* owner, const int* neigh,
+                          int n_patches, const int* patch_start, const int* patch_size,
+                          char* err, int errlen);
+void orc_mesh_free(orc_mesh* m);
+int orc_mesh_ncells(const orc_mesh* m);
+void orc_mesh_geometry(const orc_mesh* m, double* cc, double* vol, double* xf, double* nf, double* sf,
+                       double* af, double* max_nonorth);
+
+/* BC: per patch type (1 Dirichlet / 0 Neumann) for u,v,w,p and per-face values (nFaces) */
+void orc_set_bc(orc_mesh* m, const int* tu, const int* tv, const int* tw, const int* tp,
+                const double* uf, const double* vf, const double* wf, const double* pf);
+
+/* kernel_apply_lsq_gradient on the build_lsq_gradient_operator coefficients (GSV1:1159-1251,
+ * 1403-1440), field = 0 u, 1 v, 2 w, 3 p */
+void orc_lsq_gradient(const orc_mesh* m, int field, const double* phi, double* gx, double* gy, double* gz);
+
+/* momentum system for old fields (GSV1:2346-2528 and 3350-3405 with it == 1) */
+void orc_momentum(const orc_mesh* m, double rho, double mu, double u_relax, const double* u,
+                  const double* v, const double* w, const double* p, double* diag, double* a_pn,
+                  double* a_np, double* rhs3, double* rau);
+
+/* pressure matrix (GSV1:2532-2551) + Rhie-Chow flux (GSV1:1474-1521) + continuity
+ * (GSV1:1523-1536) */
+void orc_pressure(const orc_mesh* m, double rho, const double* u, const double* v, const double* w,
+                  const double* p, const double* rau, double* diag, double* a_pn, double* phi_star,
+                  double* div_star);
+
+/* nsteps SIMPLE iterations (GSV1:3388-3634).  u,v,w,p in/out, phi out (nFaces).  stats may be
+ * NULL (else nsteps entries).  Returns executed steps (early stop on convergence). */
+int orc_simple_run(orc_mesh* m, const orc_params* prm, int nsteps, double* u, double* v, double* w,
+                   double* p, double* phi, orc_stats* stats);
+
+/* compute_patch_forces_wall_shear (GSV1:2828-2933); out: Fp[3], Fv[3], F[3], area, nFaces,
+ * minDn, maxDn, maxUt, maxShear */
+void orc_patch_force(const orc_mesh* m, int patch, int normal_sign, double mu, const double* u,
+                     const double* v, const double* w, const double* p, double* out11);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
