@@ -73,6 +73,9 @@ SIGNATURES = {
     "anb_get_state": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "anb_simple_iterate": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.POINTER(IterStats), _ip]),
     "anb_patch_force": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
+    "anb_profile_select": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "anb_profile_read": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_longlong), _dp, _dp]),
+    "anb_launch_count": (ct.c_longlong, []),
     "anb_debug_gradient": (ct.c_int, [ct.c_void_p, ct.c_int, _dp, _dp, _dp, _dp]),
     "anb_debug_momentum": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "anb_debug_pressure": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
@@ -247,9 +250,10 @@ class Solver:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p)]
         self._check(lib().anb_set_state(self._h, *map(_d, arrs)))
 
-    def get_state(self) -> dict:
+    def get_state(self, with_phi: bool = True) -> dict:
         C, F = self.n_cells, self.n_faces
-        o = dict(u=np.zeros(C), v=np.zeros(C), w=np.zeros(C), p=np.zeros(C), phi=np.zeros(F))
+        o = dict(u=np.zeros(C), v=np.zeros(C), w=np.zeros(C), p=np.zeros(C))
+        o["phi"] = np.zeros(F) if with_phi else None
         self._check(lib().anb_get_state(self._h, _d(o["u"]), _d(o["v"]), _d(o["w"]), _d(o["p"]), _d(o["phi"])))
         return o
 

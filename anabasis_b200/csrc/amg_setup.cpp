@@ -15,30 +15,73 @@ struct HCsr {
   std::vector<double> val, diag;
 };
 
-// One pass of pairwise matching; returns aggregate id per row and the aggregate count.
+// One pass of pairwise aggregation by heavy-edge matching: edges (i, j) with negative coupling,
+// strength -a_ij / sqrt(a_ii a_jj), are visited strongest first and matched when both ends are
+// free and the edge is strong for either end (>= beta of that row's strongest coupling).  Rows
+// left unmatched join the aggregate of their strongest neighbour (aggregates of 2-3 rows), or
+// stay single when they have no negative coupling.  Ties break on row index, so the result is
+// deterministic.  Returns the aggregate of every row; nc receives the aggregate count, numbered
+// in order of each aggregate's first row.
 std::vector<int> pairwise(const HCsr& A, double beta, int& nc) {
-  std::vector<int> agg(A.n, -1);
+  const int n = A.n;
+  std::vector<double> rowMax(n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int k = A.off[i]; k < A.off[i + 1]; ++k) rowMax[i] = std::max(rowMax[i], -A.val[k]);
+  struct Edge {
+    double s;
+    int i, j;
+  };
+  std::vector<Edge> edges;
+  edges.reserve(A.off[n] / 2 + 1);
+  for (int i = 0; i < n; ++i)
+    for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
+      const int j = A.col[k];
+      const double a = -A.val[k];
+      if (j <= i || a <= 0.0) continue;
+      if (a < beta * rowMax[i] && a < beta * rowMax[j]) continue;
+      const double dd = std::sqrt(std::max(A.diag[i], 1e-300) * std::max(A.diag[j], 1e-300));
+      edges.push_back({a / dd, i, j});
+    }
+  std::sort(edges.begin(), edges.end(), [](const Edge& x, const Edge& y) {
+    if (x.s != y.s) return x.s > y.s;
+    if (x.i != y.i) return x.i < y.i;
+    return x.j < y.j;
+  });
+  std::vector<int> mate(n, -1);
+  for (const Edge& e : edges)
+    if (mate[e.i] < 0 && mate[e.j] < 0) {
+      mate[e.i] = e.j;
+      mate[e.j] = e.i;
+    }
+  std::vector<int> agg(n, -1);
   nc = 0;
-  for (int i = 0; i < A.n; ++i) {
-    if (agg[i] >= 0) continue;
-    double mx = 0.0;
-    for (int k = A.off[i]; k < A.off[i + 1]; ++k) mx = std::max(mx, -A.val[k]);
+  for (int i = 0; i < n; ++i) {
+    if (agg[i] >= 0 || mate[i] < 0) continue;
+    agg[i] = agg[mate[i]] = nc++;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (mate[i] >= 0) continue;
     int best = -1;
     double bestV = 0.0;
-    if (mx > 0.0) {
-      for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
-        const int j = A.col[k];
-        const double s = -A.val[k];
-        if (j == i || agg[j] >= 0 || s < beta * mx) continue;
-        if (best < 0 || s > bestV || (s == bestV && j < best)) {
-          best = j;
-          bestV = s;
-        }
+    for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
+      const int j = A.col[k];
+      const double a = -A.val[k];
+      if (j == i || a <= 0.0 || mate[j] < 0) continue;
+      if (best < 0 || a > bestV) {
+        best = j;
+        bestV = a;
       }
     }
-    agg[i] = nc;
-    if (best >= 0) agg[best] = nc;
-    ++nc;
+    agg[i] = best >= 0 ? agg[best] : -2;
+  }
+  for (int i = 0; i < n; ++i)
+    if (agg[i] == -2) agg[i] = nc++;
+  // renumber aggregates in order of their first row (keeps the coarse ordering banded)
+  std::vector<int> ren(nc, -1);
+  int next = 0;
+  for (int i = 0; i < n; ++i) {
+    if (ren[agg[i]] < 0) ren[agg[i]] = next++;
+    agg[i] = ren[agg[i]];
   }
   return agg;
 }

@@ -97,6 +97,7 @@ struct anb_ctx {
   // pinned host mirrors
   int* hFlags = nullptr;
   double* hScal = nullptr;
+  double* hStage = nullptr;   // 3 * nCells staging for cell fields
   // state
   bool bcSet = false, stateSet = false, pZeroBC = true;
   long long outerStep = 0;
@@ -105,6 +106,9 @@ struct anb_ctx {
   bool amgBuilt = false;
   AmgDev amg;
   std::vector<AmgLevelHost> amgHost;
+  // measurement
+  Prof prof;
+  AlgoBytes ab;
 };
 
 namespace {
@@ -143,21 +147,35 @@ void permute_in(const anb_ctx* c, const double* src, std::vector<double>& dst, i
     for (int r = 0; r < c->C; ++r) dst[(size_t)q * c->C + r] = src[(size_t)q * c->C + c->L.new2old[r]];
 }
 
+// Cell fields cross the host/device boundary through a pinned staging buffer (3 * nCells):
+// the host permutes into / out of it, the copy engine moves it with one DMA.
 void upload_cells(anb_ctx* c, const double* const* src, double* dst, int comps) {
-  std::vector<double> h((size_t)comps * c->C);
-  for (int q = 0; q < comps; ++q)
-    for (int r = 0; r < c->C; ++r) h[(size_t)q * c->C + r] = src[q][c->L.new2old[r]];
-  CK(cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  double* h = c->hStage;
+  const int* n2o = c->L.new2old.data();
+  const int C = c->C;
+  for (int q = 0; q < comps; ++q) {
+    const double* s = src[q];
+    double* d = h + (size_t)q * C;
+#pragma omp parallel for schedule(static) if (C > 200000)
+    for (int r = 0; r < C; ++r) d[r] = s[n2o[r]];
+  }
+  CK(cudaMemcpyAsync(dst, h, (size_t)comps * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
 }
 
 void download_cells(anb_ctx* c, const double* src, double* const* dst, int comps) {
-  std::vector<double> h((size_t)comps * c->C);
-  CK(cudaMemcpyAsync(h.data(), src, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  double* h = c->hStage;
+  const int* n2o = c->L.new2old.data();
+  const int C = c->C;
+  CK(cudaMemcpyAsync(h, src, (size_t)comps * C * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int q = 0; q < comps; ++q)
-    if (dst[q])
-      for (int r = 0; r < c->C; ++r) dst[q][c->L.new2old[r]] = h[(size_t)q * c->C + r];
+  for (int q = 0; q < comps; ++q) {
+    double* d = dst[q];
+    if (!d) continue;
+    const double* s = h + (size_t)q * C;
+#pragma omp parallel for schedule(static) if (C > 200000)
+    for (int r = 0; r < C; ++r) d[n2o[r]] = s[r];
+  }
 }
 
 // Face array on the device (new order, new orientation) -> input order and orientation.
@@ -504,6 +522,7 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   CK(cudaMemcpyAsync(c->hScal, c->stats, sizeof(double) * 9, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
+  c->prof.flush();
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
@@ -627,6 +646,12 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     CK(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, prm->device));
     c->lc.stream = c->stream;
     c->lc.rowBlocks = std::max(1, std::min((c->C + kBlock - 1) / kBlock, nSM * 8));
+    c->lc.prof = &c->prof;
+    c->lc.ab = &c->ab;
+    c->ab.C = c->C;
+    c->ab.Fi = c->nI;
+    c->ab.Fb = c->nB;
+    c->ab.nnzOff = 2LL * c->nI;
 
     DevArena& A = c->arena;
     // faces
@@ -717,6 +742,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     CK(cudaMemset(c->Pc, 0, sizeof(double) * C));
     CK(cudaMallocHost(&c->hFlags, sizeof(int) * 32));
     CK(cudaMallocHost(&c->hScal, sizeof(double) * 64));
+    CK(cudaMallocHost(&c->hStage, sizeof(double) * 3 * C));
     return ANB_OK;
   });
   if (rc != ANB_OK) {
@@ -725,6 +751,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->hFlags) cudaFreeHost(c->hFlags);
     if (c->hScal) cudaFreeHost(c->hScal);
+  if (c->hStage) cudaFreeHost(c->hStage);
     return rc;
   }
   *out = c.release();
@@ -739,6 +766,7 @@ void anb_destroy(anb_ctx* c) {
   c->arena.release();
   if (c->hFlags) cudaFreeHost(c->hFlags);
   if (c->hScal) cudaFreeHost(c->hScal);
+  if (c->hStage) cudaFreeHost(c->hStage);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -874,6 +902,26 @@ int anb_patch_force(anb_ctx* c, int patch, int sign, anb_force_report* out) {
     out->max_shear_mag = h[14];
     return ANB_OK;
   });
+}
+
+long long anb_launch_count(void) { return g_launches.load(); }
+
+int anb_profile_select(anb_ctx* c, int family) {
+  if (!c || family < 0 || family > kKfAmgLevel0) return ANB_ERR_INVALID;
+  c->prof.flush();
+  c->prof.family = family;
+  c->prof.launches = 0;
+  c->prof.seconds = 0.0;
+  c->prof.bytes = 0.0;
+  return ANB_OK;
+}
+
+int anb_profile_read(anb_ctx* c, long long* launches, double* seconds, double* bytes) {
+  if (!c) return ANB_ERR_INVALID;
+  if (launches) *launches = c->prof.launches;
+  if (seconds) *seconds = c->prof.seconds;
+  if (bytes) *bytes = c->prof.bytes;
+  return ANB_OK;
 }
 
 int anb_debug_gradient(anb_ctx* c, int field, const double* phi, double* gx, double* gy, double* gz) {

@@ -3,11 +3,84 @@
 
 #include "device.cuh"
 
+#include <atomic>
+#include <vector>
+
 namespace anb {
 
+// Kernel families that can be timed with CUDA events (anb_profile_select in include/anb.h).
+enum KernelFamily {
+  kKfNone = 0, kKfGradient = 1, kKfMomentum = 2, kKfPressureRc = 3, kKfNonOrth = 4, kKfFluxFinal = 5,
+  kKfBicgSpmv = 6, kKfPcgSpmv = 7, kKfAmgLevel0 = 8
+};
+
+// Event-pair recorder for one selected kernel family on one stream.
+struct Prof {
+  int family = kKfNone;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  long long launches = 0;
+  double seconds = 0.0, bytes = 0.0;
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  // call after the stream is synchronized
+  void flush() {
+    for (size_t k = 0; k + 1 < used; k += 2) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, pool[k], pool[k + 1]) == cudaSuccess) seconds += ms * 1e-3;
+    }
+    used = 0;
+  }
+  ~Prof() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
+extern std::atomic<long long> g_launches;
+
+struct AlgoBytes;
 struct LaunchCfg {
   int rowBlocks;   // grid for row-parallel kernels (grid-stride)
   cudaStream_t stream;
+  Prof* prof = nullptr;
+  const AlgoBytes* ab = nullptr;
+};
+
+// Records a start/stop event pair around the launches in its scope when `fam` is selected.
+struct ProfScope {
+  const LaunchCfg& lc;
+  bool on;
+  ProfScope(const LaunchCfg& l, int fam, double bytes, int nLaunch = 1) : lc(l) {
+    g_launches += nLaunch;
+    on = lc.prof && lc.prof->family == fam;
+    if (on) {
+      cudaEventRecord(lc.prof->next(), lc.stream);
+      lc.prof->launches += 1;
+      lc.prof->bytes += bytes;
+    }
+  }
+  ~ProfScope() {
+    if (on) cudaEventRecord(lc.prof->next(), lc.stream);
+  }
+};
+
+// Algorithmic (compulsory) bytes of one launch, used for the roofline report.
+struct AlgoBytes {
+  double gradient(int nf) const;
+  double momentum() const;
+  double pressure_rc() const;
+  double nonorth() const;
+  double flux_final() const;
+  double bicg_spmv(int nc) const;
+  double pcg_spmv() const;
+  int C = 0, Fi = 0, Fb = 0;
+  long long nnzOff = 0;
 };
 
 // Least-squares gradients of up to four cell fields.  fieldBit selects the Dirichlet bit in

@@ -424,26 +424,52 @@ __global__ void k_patch_force(DMesh m, int b0, int b1, int sign, double mu, cons
 
 }  // namespace
 
+std::atomic<long long> g_launches{0};
+
+// Compulsory bytes: every array element read or written once (index arrays included, SELL padding
+// and the second visit of a face from its other cell excluded).
+double AlgoBytes::gradient(int nf) const {
+  return C * (48.0 + 24.0 + 8.0 * nf + 24.0 * nf) + nnzOff * 8.0 + 4.0 * (C + 1) + Fb * (4.0 + 1.0 + 24.0 + 8.0 * nf);
+}
+double AlgoBytes::momentum() const {
+  return C * (8.0 + 24 + 24 + 96 + 8 + 24 + 8) + Fi * 65.0 + nnzOff * 16.0 + 4.0 * (C + 1) + Fb * (80.0 + 1 + 24 + 4);
+}
+double AlgoBytes::pressure_rc() const {
+  return C * 96.0 + Fi * (65.0 + 8) + nnzOff * 16.0 + 4.0 * (C + 1) + Fb * (80.0 + 1 + 24 + 8 + 4);
+}
+double AlgoBytes::nonorth() const { return C * 48.0 + Fi * 65.0 + nnzOff * 8.0 + 4.0 * (C + 1) + Fb * (80.0 + 1 + 4); }
+double AlgoBytes::flux_final() const {
+  return C * 136.0 + Fi * (65.0 + 16) + nnzOff * 8.0 + 4.0 * (C + 1) + Fb * (80.0 + 1 + 8 + 8 + 8 + 4);
+}
+double AlgoBytes::bicg_spmv(int nc) const { return 8.0 * C + 12.0 * nnzOff + 24.0 * nc * C; }
+double AlgoBytes::pcg_spmv() const { return 40.0 * C + 12.0 * nnzOff; }
+
 void launch_lsq_grad(const LaunchCfg& lc, const DMesh& m, const GradArgs& a) {
+  ProfScope ps(lc, kKfGradient, lc.ab ? lc.ab->gradient(a.nf) : 0.0);
   if (a.nf == 4) k_lsq_grad<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else if (a.nf == 3) k_lsq_grad<3><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else if (a.nf == 2) k_lsq_grad<2><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else k_lsq_grad<1><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgs& a) {
+  ProfScope ps(lc, kKfMomentum, lc.ab ? lc.ab->momentum() : 0.0);
   k_momentum<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgs& a) {
+  ProfScope ps(lc, kKfPressureRc, lc.ab ? lc.ab->pressure_rc() : 0.0);
   k_pressure_rc<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_nonorth_rhs(const LaunchCfg& lc, const DMesh& m, const NonOrthArgs& a) {
+  ProfScope ps(lc, kKfNonOrth, lc.ab ? lc.ab->nonorth() : 0.0);
   k_nonorth_rhs<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a) {
+  ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0);
   k_flux_final<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_patch_force(cudaStream_t s, const DMesh& m, int b0, int b1, int sign, double mu, const double* bA,
                         const double* bN, const double* U, const double* P, double* out) {
+  g_launches += 1;
   k_patch_force<<<1, 512, 0, s>>>(m, b0, b1, sign, mu, bA, bN, U, P, out);
 }
 

@@ -481,22 +481,34 @@ __global__ void k_amg_dense_factor(AmgLevelDev c, double* inv) {
 }  // namespace
 
 void bicg_init(const LaunchCfg& lc, const BicgArgs& a) {
+  g_launches += 1;
   k_bicg_init<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
 void bicg_iteration(const LaunchCfg& lc, const BicgArgs& a) {
+  g_launches += 3;
   k_bicg_p<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-  k_bicg_v<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  {
+    ProfScope ps(lc, kKfBicgSpmv, lc.ab ? lc.ab->bicg_spmv(a.nc) : 0.0);
+    k_bicg_v<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
   k_bicg_s<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-  k_bicg_t<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  {
+    ProfScope ps(lc, kKfBicgSpmv, lc.ab ? lc.ab->bicg_spmv(a.nc) : 0.0);
+    k_bicg_t<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
   k_bicg_x<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
 
-void pcg_init(const LaunchCfg& lc, const PcgArgs& a) { k_pcg_init<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a); }
+void pcg_init(const LaunchCfg& lc, const PcgArgs& a) {
+  g_launches += 1;
+  k_pcg_init<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+}
 
 static int blocks_for(int n, int cap) { return std::max(1, std::min(cap, (n + kBlock - 1) / kBlock)); }
 
 static void vcycle(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
   const int L = amg->nLevels;
+  g_launches += 2 * L - 1;
   // level 0 right-hand side is the PCG residual
   for (int l = 0; l + 1 < L; ++l) {
     const AmgLevelDev& f = amg->lv[l];
@@ -515,14 +527,22 @@ static void vcycle(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
 }
 
 void pcg_precondition(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
-  if (!amg || amg->nLevels < 2) k_pcg_jacobi<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-  else vcycle(lc, a, amg);
+  if (!amg || amg->nLevels < 2) {
+    g_launches += 1;
+    k_pcg_jacobi<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  } else {
+    vcycle(lc, a, amg);
+  }
 }
 
 void pcg_iteration(const LaunchCfg& lc, const PcgArgs& a, int it, const AmgDev* amg) {
   const double* pOld = (it & 1) ? a.p1 : a.p0;
   double* pNew = (it & 1) ? a.p0 : a.p1;
-  k_pcg_pq<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+  {
+    ProfScope ps(lc, kKfPcgSpmv, lc.ab ? lc.ab->pcg_spmv() : 0.0);
+    k_pcg_pq<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+  }
+  g_launches += 1;
   k_pcg_xr<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pNew);
   pcg_precondition(lc, a, amg);
 }
@@ -531,11 +551,13 @@ void amg_refresh(const LaunchCfg& lc, AmgDev& amg) {
   for (int l = 0; l + 1 < amg.nLevels; ++l) {
     AmgLevelDev& f = amg.lv[l];
     AmgLevelDev& c = amg.lv[l + 1];
+    g_launches += 1;
     k_amg_galerkin<<<blocks_for(f.nEntNext + f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(f, c.val, c.diag);
   }
   const AmgLevelDev& c = amg.lv[amg.nLevels - 1];
   const size_t smem = sizeof(double) * (size_t)c.n * c.n;
   cudaFuncSetAttribute(k_amg_dense_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  g_launches += 1;
   k_amg_dense_factor<<<1, 1024, smem, lc.stream>>>(c, amg.dense);
 }
 

@@ -129,6 +129,22 @@ int anb_simple_iterate(anb_ctx* ctx, int nsteps, double tol_mass, double tol_vel
  * patch is the 0-based patch index in input order. */
 int anb_patch_force(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* out);
 
+/* ---- measurement (no counterpart in the reference; used by the benchmark) ------------------
+ * Kernel families for anb_profile_select: every launch of the selected family is bracketed by
+ * CUDA events on the context's stream and its algorithmic (compulsory) bytes are accumulated. */
+#define ANB_KF_NONE 0
+#define ANB_KF_GRADIENT 1      /* least-squares gradient            */
+#define ANB_KF_MOMENTUM 2      /* momentum assembly                  */
+#define ANB_KF_PRESSURE_RC 3   /* pressure matrix + Rhie-Chow flux   */
+#define ANB_KF_NONORTH 4       /* non-orthogonal pressure rhs        */
+#define ANB_KF_FLUX_FINAL 5    /* flux/velocity correction           */
+#define ANB_KF_BICG_SPMV 6     /* BiCGSTAB matrix-vector products    */
+#define ANB_KF_PCG_SPMV 7      /* PCG matrix-vector product          */
+int anb_profile_select(anb_ctx* ctx, int family);
+int anb_profile_read(anb_ctx* ctx, long long* launches, double* seconds, double* algo_bytes);
+/* Number of kernel launches this process has issued through libanb.so. */
+long long anb_launch_count(void);
+
 /* ---- diagnostic entry points (parity tests of single stages) --------------------------------
  * Each runs one stage of the outer iteration on the given host fields (input numbering) and
  * returns its output in input numbering.  Internal-face coefficients are reported per face in
