@@ -122,36 +122,6 @@ HCsr galerkin(const HCsr& A, const std::vector<int>& agg, int nc) {
   return C;
 }
 
-void to_sell(const HCsr& A, AmgLevelHost& lv, std::vector<int>& csrToSell) {
-  lv.n = A.n;
-  lv.nSlices = (A.n + kSlice - 1) / kSlice;
-  lv.sliceOff.assign(lv.nSlices + 1, 0);
-  lv.rowLen.resize(A.n);
-  for (int i = 0; i < A.n; ++i) lv.rowLen[i] = A.off[i + 1] - A.off[i];
-  for (int s = 0; s < lv.nSlices; ++s) {
-    int w = 0;
-    for (int r = s * kSlice; r < std::min(A.n, (s + 1) * kSlice); ++r) w = std::max(w, lv.rowLen[r]);
-    lv.sliceOff[s + 1] = lv.sliceOff[s] + w * kSlice;
-  }
-  lv.col.assign(lv.sliceOff[lv.nSlices], 0);
-  csrToSell.assign(A.off[A.n], 0);
-  for (int s = 0; s < lv.nSlices; ++s) {
-    const int w = (lv.sliceOff[s + 1] - lv.sliceOff[s]) / kSlice;
-    for (int lane = 0; lane < kSlice; ++lane) {
-      const int r = s * kSlice + lane;
-      for (int k = 0; k < w; ++k) {
-        const int e = lv.sliceOff[s] + k * kSlice + lane;
-        if (r < A.n && k < lv.rowLen[r]) {
-          lv.col[e] = A.col[A.off[r] + k];
-          csrToSell[A.off[r] + k] = e;
-        } else {
-          lv.col[e] = r < A.n ? r : 0;
-        }
-      }
-    }
-  }
-}
-
 }  // namespace
 
 std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector<double>& vals,
@@ -178,7 +148,6 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
   {
     AmgLevelHost lv0;
     lv0.n = A.n;
-    lv0.nSlices = L.nSlices;
     levels.push_back(std::move(lv0));  // pattern comes from the mesh layout
   }
   while ((int)levels.size() < opt.maxLevels && A.n > opt.coarseMax) {
@@ -208,10 +177,11 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
       for (int i = 0; i < A.n; ++i) fine.mem[fill[agg[i]]++] = i;
     }
     AmgLevelHost coarse;
-    std::vector<int> cCsrToSell;
-    to_sell(Cc, coarse, cCsrToSell);
-    // gather lists: coarse SELL entries then coarse diagonals
-    const int nEnt = coarse.sliceOff[coarse.nSlices];
+    coarse.n = nc;
+    coarse.rowOff = Cc.off;
+    coarse.col = Cc.col;
+    // gather lists: coarse CSR entries then coarse diagonals
+    const int nEnt = Cc.off[nc];
     std::vector<int> cnt(nEnt + nc + 1, 0);
     std::vector<int> target(A.off[A.n]);
     for (int i = 0; i < A.n; ++i) {
@@ -219,12 +189,11 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
       for (int k = A.off[i]; k < A.off[i + 1]; ++k) {
         const int J = agg[A.col[k]];
         int t;
-        if (J == I) t = nEnt + I;
-        else {
-          const int* b = &Cc.col[Cc.off[I]];
-          const int* e = &Cc.col[Cc.off[I + 1]];
-          const int* it = std::lower_bound(b, e, J);
-          t = cCsrToSell[Cc.off[I] + (int)(it - &Cc.col[0]) - Cc.off[I]];
+        if (J == I) {
+          t = nEnt + I;
+        } else {
+          const auto b = Cc.col.begin() + Cc.off[I], e = Cc.col.begin() + Cc.off[I + 1];
+          t = (int)(std::lower_bound(b, e, J) - Cc.col.begin());
         }
         target[k] = t;
         cnt[t + 1]++;
@@ -242,9 +211,10 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
       }
     }
     levels.push_back(std::move(coarse));
-    // next level's CSR with storage indices of the coarse SELL
+    // the coarse level is stored as CSR: its storage index is the CSR index
     A = std::move(Cc);
-    storage = cCsrToSell;
+    storage.resize(A.off[A.n]);
+    for (int k = 0; k < A.off[A.n]; ++k) storage[k] = k;
   }
   return levels;
 }

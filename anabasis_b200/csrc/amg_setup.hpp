@@ -20,9 +20,9 @@ namespace anb {
 
 struct AmgLevelHost {
   int n = 0;
-  // SELL-32 off-diagonal pattern of this level (level 0 uses the mesh layout's pattern)
-  int nSlices = 0;
-  std::vector<int> sliceOff, col, rowLen;
+  // CSR off-diagonal pattern of this level (levels >= 1; level 0 uses the mesh layout's SELL-32
+  // pattern).  Coarse rows are long and few, so the device walks them with several lanes per row.
+  std::vector<int> rowOff, col;
   // restriction to the next level (empty on the coarsest level)
   int nc = 0;
   std::vector<int> agg;            // n: aggregate (coarse row) of each row

@@ -247,7 +247,7 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
       CK(cudaMemcpyAsync(a.fl + 4 * q, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
     }
   int done = 0;
-  int batch = std::max(2, std::min(c->lastMomIts, 32));
+  int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
   while (true) {
     for (int k = 0; k < batch; ++k) bicg_iteration(c->lc, a);
     done += batch;
@@ -255,7 +255,7 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
     bool all = true;
     for (int q = 0; q < 3; ++q) all = all && c->hFlags[4 * q];
     if (all || done > a.maxit + 2) break;
-    batch = 4;
+    batch = 2;
   }
   int mx = 0;
   for (int q = 0; q < 3; ++q) {
@@ -264,12 +264,25 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
     mx = std::max(mx, its[q]);
   }
   c->lastMomIts = std::max(1, mx);
+  if (c->prof.family == kKfBicgSpmv) {  // count only the components each launch worked on
+    double booked = 2.0 * done * c->ab.bicg_spmv(3), real = 0.0;
+    long long realLaunches = 0;
+    for (int k = 1; k <= done; ++k) {
+      int n = 0;
+      for (int q = 0; q < 3; ++q) n += its[q] >= k ? 1 : 0;
+      if (n > 0) {
+        real += 2.0 * c->ab.bicg_spmv(n);
+        realLaunches += 2;
+      }
+    }
+    c->prof.bytes += real - booked;
+    c->prof.launches += realLaunches - 2LL * done;
+  }
 }
 
 void ensure_amg(anb_ctx* c);
 
-// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
-void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+PcgArgs pcg_args(anb_ctx* c, const double* b, double* x, double rtol) {
   PcgArgs a{};
   a.A = p_sell(c);
   a.b = b;
@@ -281,21 +294,34 @@ void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* it
   a.rtol = rtol;
   a.maxit = c->prm.p_maxit;
   a.red = c->red;
+  return a;
+}
+
+// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
+void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  PcgArgs a = pcg_args(c, b, x, rtol);
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
   if (amg) c->amg.lv[0].b = c->pr;
   pcg_init(c->lc, a);
   pcg_precondition(c->lc, a, amg);
+  // enqueue most of the expected iterations (previous solve's count) before the first poll,
+  // then poll in small batches; iterations after convergence return at once
   int it = 0;
-  int batch = std::max(2, std::min(c->lastPIts, 64));
+  int batch = std::max(2, std::min(3 * c->lastPIts / 4, 64));
+  const int tail = std::max(2, c->lastPIts / 8);
   while (true) {
     for (int k = 0; k < batch; ++k) pcg_iteration(c->lc, a, it++, amg);
     poll(c, a.fl, 4);
     if (c->hFlags[0] || it > a.maxit + 2) break;
-    batch = std::max(2, std::min(8, batch / 2 + 1));
+    batch = tail;
   }
   *its = c->hFlags[1];
   *conv = c->hFlags[2] != 0;
   c->lastPIts = std::max(1, *its);
+  if (c->prof.family == kKfPcgSpmv) {  // launches after convergence returned at once: not counted
+    c->prof.bytes -= (double)(it - *its) * c->ab.pcg_spmv();
+    c->prof.launches -= it - *its;
+  }
 }
 
 void ensure_amg(anb_ctx* c) {
@@ -322,9 +348,9 @@ void ensure_amg(anb_ctx* c) {
         d.val = c->pval;
         d.diag = c->pdiag;
       } else {
-        d.sliceOff = ar.upload(h.sliceOff);
+        d.rowOff = ar.upload(h.rowOff);
         d.col = ar.upload(h.col);
-        d.val = ar.alloc<double>(h.sliceOff.back());
+        d.val = ar.alloc<double>(h.rowOff.back());
         d.diag = ar.alloc<double>(h.n);
         d.b = ar.alloc<double>(h.n);
       }
@@ -336,7 +362,7 @@ void ensure_amg(anb_ctx* c) {
         d.mem = ar.upload(h.mem);
         d.gOff = ar.upload(h.gOff);
         d.gIdx = ar.upload(h.gIdx);
-        d.nEntNext = c->amgHost[l + 1].sliceOff.back();
+        d.nEntNext = c->amgHost[l + 1].rowOff.back();
       }
     }
     const int nd = c->amgHost.back().n;
@@ -344,6 +370,11 @@ void ensure_amg(anb_ctx* c) {
     A.nDense = nd;
     A.dense = ar.alloc<double>((size_t)nd * nd);
     c->amgBuilt = true;
+    const char* noGraph = std::getenv("ANB_NO_GRAPH");
+    if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) {
+      A.lv[0].b = c->pr;
+      CK(amg_capture_graph(c->lc, pcg_args(c, c->pb, c->Pc, 0.0), A));
+    }
   }
   if (c->amg.nLevels >= 2) amg_refresh(c->lc, c->amg);
 }
@@ -762,6 +793,7 @@ void anb_destroy(anb_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->prm.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
   c->amgArena.release();
   c->arena.release();
   if (c->hFlags) cudaFreeHost(c->hFlags);
@@ -907,7 +939,7 @@ int anb_patch_force(anb_ctx* c, int patch, int sign, anb_force_report* out) {
 long long anb_launch_count(void) { return g_launches.load(); }
 
 int anb_profile_select(anb_ctx* c, int family) {
-  if (!c || family < 0 || family > kKfAmgLevel0) return ANB_ERR_INVALID;
+  if (!c || family < 0 || family >= kKfCount) return ANB_ERR_INVALID;
   c->prof.flush();
   c->prof.family = family;
   c->prof.launches = 0;

@@ -11,7 +11,8 @@ namespace anb {
 // Kernel families that can be timed with CUDA events (anb_profile_select in include/anb.h).
 enum KernelFamily {
   kKfNone = 0, kKfGradient = 1, kKfMomentum = 2, kKfPressureRc = 3, kKfNonOrth = 4, kKfFluxFinal = 5,
-  kKfBicgSpmv = 6, kKfPcgSpmv = 7, kKfAmgLevel0 = 8
+  kKfBicgSpmv = 6, kKfPcgSpmv = 7, kKfAmgResid0 = 8, kKfAmgUp0 = 9, kKfAmgCoarse = 10, kKfPcgUpdate = 11,
+  kKfBicgVector = 12, kKfCount = 13
 };
 
 // Event-pair recorder for one selected kernel family on one stream.
@@ -191,8 +192,10 @@ void pcg_precondition(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg);
 // ---- AMG (aggregation, V-cycle) ------------------------------------------------------------
 struct AmgLevelDev {
   int n, nc;
-  // matrix of this level (level 0 borrows the pressure matrix)
+  // matrix of this level: level 0 borrows the pressure matrix (SELL-32 slices in sliceOff),
+  // coarser levels are CSR (rowOff)
   const int* sliceOff;
+  const int* rowOff;
   const int* col;
   double* val;
   double* diag;
@@ -213,7 +216,10 @@ struct AmgDev {
   int nDense = 0;
   double omega = 0.6667;     // Jacobi weight
   double corr = 1.0;         // coarse-correction scaling
+  cudaGraphExec_t graph = nullptr;  // captured V-cycle (see amg_capture_graph)
+  int graphKernels = 0;
 };
 void amg_refresh(const LaunchCfg& lc, AmgDev& amg);  // Galerkin values + dense inverse
+cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgs& a, AmgDev& amg);
 
 }  // namespace anb

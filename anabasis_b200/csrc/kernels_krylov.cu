@@ -7,6 +7,8 @@
 // convergence flags.  Kernels return immediately once their system is converged, so the host
 // can enqueue several iterations between polls without changing the arithmetic.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 #include "kernels.cuh"
 
@@ -19,11 +21,30 @@ __device__ __forceinline__ double sell_row(const DSell& A, int r, const double* 
   const int b = __ldg(&A.sliceOff[s]) + (r & 31);
   const int W = (__ldg(&A.sliceOff[s + 1]) - __ldg(&A.sliceOff[s])) >> 5;
   double y = A.diag[r] * x[r];
+#pragma unroll 4
   for (int k = 0; k < W; ++k) {
     const int e = b + (k << 5);
-    y += A.val[e] * x[__ldg(&A.col[e])];
+    y += __ldg(&A.val[e]) * x[__ldg(&A.col[e])];
   }
   return y;
+}
+
+// y_c = (D + Off) x_c for up to three vectors sharing one pass over the matrix row
+__device__ __forceinline__ void sell_row3(const DSell& A, int r, const double* x, size_t n, const bool* act, int nc,
+                                          double* y) {
+  const int s = r >> 5;
+  const int b = __ldg(&A.sliceOff[s]) + (r & 31);
+  const int W = (__ldg(&A.sliceOff[s + 1]) - __ldg(&A.sliceOff[s])) >> 5;
+  const double d = A.diag[r];
+  for (int c = 0; c < 3; ++c) y[c] = (c < nc && act[c]) ? d * x[c * n + r] : 0.0;
+#pragma unroll 2
+  for (int k = 0; k < W; ++k) {
+    const int e = b + (k << 5);
+    const double v = __ldg(&A.val[e]);
+    const int j = __ldg(&A.col[e]);
+    for (int c = 0; c < 3; ++c)
+      if (c < nc && act[c]) y[c] += v * x[c * n + j];
+  }
 }
 
 // ---------------------------------------------------------------- BiCGSTAB, nc components
@@ -104,12 +125,13 @@ __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgs a) {
   for (int c = 0; c < a.nc; ++c) act[c] = !a.fl[4 * c];
   double acc[3] = {0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double y[3];
+    sell_row3(a.A, r, a.ph, (size_t)n, act, a.nc, y);
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
-      const double vv = sell_row(a.A, r, a.ph + o);
-      a.v[o + r] = vv;
-      acc[c] += a.rh[o + r] * vv;
+      a.v[o + r] = y[c];
+      acc[c] += a.rh[o + r] * y[c];
     }
   }
   if (grid_reduce<3>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
@@ -166,10 +188,12 @@ __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgs a) {
   for (int c = 0; c < a.nc; ++c) act[c] = !a.fl[4 * c] && !a.fl[4 * c + 1];
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double y[3];
+    sell_row3(a.A, r, a.sh, (size_t)n, act, a.nc, y);
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
-      const double tv = sell_row(a.A, r, a.sh + o);
+      const double tv = y[c];
       a.t[o + r] = tv;
       acc[2 * c] += tv * a.s[o + r];
       acc[2 * c + 1] += tv * tv;
@@ -334,29 +358,103 @@ __global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgs a, const double* p) {
 }
 
 // ---------------------------------------------------------------- AMG V-cycle
-// Down: weighted-Jacobi pre-smoothing from zero (x = w D^-1 b) fused with the residual and
-// its piecewise-constant restriction; thread per aggregate.
-__global__ void __launch_bounds__(kBlock) k_amg_down(const int* done, AmgLevelDev f, double omega, double* bNext) {
+// Down, part 1: weighted-Jacobi pre-smoothing from zero (x = w D^-1 b) fused with the residual
+// r = b - A x (neighbour x computed on the fly); thread per row, SELL-coalesced.  r goes to x2,
+// which is free until the up sweep.
+__global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelDev f, double omega) {
+  if (*done) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
+    const double di = __ldg(&f.diag[i]);
+    const double bi = __ldg(&f.b[i]);
+    const double xi = omega * bi / di;
+    double ax = di * xi;
+    const int s = i >> 5;
+    const int b = __ldg(&f.sliceOff[s]) + (i & 31);
+    const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
+#pragma unroll 4
+    for (int k = 0; k < W; ++k) {
+      const int e = b + (k << 5);
+      const int j = __ldg(&f.col[e]);
+      ax += __ldg(&f.val[e]) * (omega * __ldg(&f.b[j]) / __ldg(&f.diag[j]));
+    }
+    f.x[i] = xi;
+    f.x2[i] = bi - ax;
+  }
+}
+
+// Coarse levels (CSR): G consecutive lanes share one row, each lane takes every G-th entry, and
+// the partial sums meet through warp shuffles.  Coarse rows are long and there are few of them,
+// so splitting rows keeps enough loads in flight.  The warp-level loop bound keeps every lane of
+// a warp in the shuffles.
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o, G);
+  return v;
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLevelDev f, double omega) {
+  if (*done) return;
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int rowsPerWarp = 32 / G;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = warp * rowsPerWarp; base < f.n; base += nWarps * rowsPerWarp) {
+    const int i = base + lane / G;
+    double acc = 0.0;
+    if (i < f.n) {
+      const int k1 = __ldg(&f.rowOff[i + 1]);
+      for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
+        const int j = __ldg(&f.col[k]);
+        acc += __ldg(&f.val[k]) * (omega * __ldg(&f.b[j]) / __ldg(&f.diag[j]));
+      }
+    }
+    acc = group_sum<G>(acc);
+    if (i < f.n && sub == 0) {
+      const double di = __ldg(&f.diag[i]), bi = __ldg(&f.b[i]);
+      const double xi = omega * bi / di;
+      f.x[i] = xi;
+      f.x2[i] = bi - di * xi - acc;
+    }
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevelDev f, const double* e, double omega,
+                                                       double corr, double* out) {
+  if (*done) return;
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int rowsPerWarp = 32 / G;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nWarps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = warp * rowsPerWarp; base < f.n; base += nWarps * rowsPerWarp) {
+    const int i = base + lane / G;
+    double acc = 0.0;
+    if (i < f.n) {
+      const int k1 = __ldg(&f.rowOff[i + 1]);
+      for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
+        const int j = __ldg(&f.col[k]);
+        acc += __ldg(&f.val[k]) * (__ldg(&f.x[j]) + corr * __ldg(&e[__ldg(&f.agg[j])]));
+      }
+    }
+    acc = group_sum<G>(acc);
+    if (i < f.n && sub == 0) {
+      const double di = __ldg(&f.diag[i]);
+      const double xi = __ldg(&f.x[i]) + corr * __ldg(&e[__ldg(&f.agg[i])]);
+      out[i] = xi + omega * (__ldg(&f.b[i]) - di * xi - acc) / di;
+    }
+  }
+}
+
+// Down, part 2: piecewise-constant restriction b_next[I] = sum of r over the rows of I.
+__global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLevelDev f, double* bNext) {
   if (*done) return;
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < f.nc; I += gridDim.x * blockDim.x) {
     double acc = 0.0;
-    const int m0 = f.memOff[I], m1 = f.memOff[I + 1];
-    for (int mm = m0; mm < m1; ++mm) {
-      const int i = f.mem[mm];
-      const double di = f.diag[i];
-      const double xi = omega * f.b[i] / di;
-      f.x[i] = xi;
-      double ax = di * xi;
-      const int s = i >> 5;
-      const int b = __ldg(&f.sliceOff[s]) + (i & 31);
-      const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
-      for (int k = 0; k < W; ++k) {
-        const int e = b + (k << 5);
-        const int j = __ldg(&f.col[e]);
-        ax += f.val[e] * (omega * f.b[j] / f.diag[j]);
-      }
-      acc += f.b[i] - ax;
-    }
+    const int m1 = __ldg(&f.memOff[I + 1]);
+#pragma unroll 4
+    for (int mm = __ldg(&f.memOff[I]); mm < m1; ++mm) acc += f.x2[__ldg(&f.mem[mm])];
     bNext[I] = acc;
   }
 }
@@ -370,18 +468,20 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
   if (*doneFlag) return;
   double acc[1] = {0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
-    const double di = f.diag[i];
-    const double xi = f.x[i] + corr * e[f.agg[i]];
+    const double di = __ldg(&f.diag[i]);
+    const double xi = __ldg(&f.x[i]) + corr * __ldg(&e[__ldg(&f.agg[i])]);
     double ax = di * xi;
     const int s = i >> 5;
     const int b = __ldg(&f.sliceOff[s]) + (i & 31);
     const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
+    // unrolled so the col -> agg -> e load chains of several entries are in flight together
+#pragma unroll 4
     for (int k = 0; k < W; ++k) {
       const int ee = b + (k << 5);
       const int j = __ldg(&f.col[ee]);
-      ax += f.val[ee] * (f.x[j] + corr * e[f.agg[j]]);
+      ax += __ldg(&f.val[ee]) * (__ldg(&f.x[j]) + corr * __ldg(&e[__ldg(&f.agg[j])]));
     }
-    const double xn = xi + omega * (f.b[i] - ax) / di;
+    const double xn = xi + omega * (__ldg(&f.b[i]) - ax) / di;
     out[i] = xn;
     if (finest) acc[0] += f.b[i] * xn;
   }
@@ -393,13 +493,17 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
   }
 }
 
-// Coarsest level: x = A^-1 b with the stored dense inverse (one block).
+// Coarsest level: x = A^-1 b with the stored dense inverse (one block).  The inverse of the SPD
+// coarse matrix is symmetric, so thread i walks column i: consecutive threads read consecutive
+// addresses.
 __global__ void k_amg_dense_apply(const int* done, int n, const double* inv, const double* b, double* x) {
   if (*done) return;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = w; i < n; i += nw) {  // warp per row, lanes across the row (coalesced)
     double s = 0.0;
-    for (int j = 0; j < n; ++j) s += inv[(size_t)i * n + j] * b[j];
-    x[i] = s;
+    for (int j = lane; j < n; j += 32) s += __ldg(&inv[(size_t)i * n + j]) * __ldg(&b[j]);
+    s = warp_sum(s);
+    if (lane == 0) x[i] = s;
   }
 }
 
@@ -425,15 +529,11 @@ __global__ void k_amg_dense_factor(AmgLevelDev c, double* inv) {
   const int n = c.n;
   for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = 0.0;
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {  // the coarsest level is always CSR
     A[i * n + i] = c.diag[i];
-    const int s = i >> 5;
-    const int b = c.sliceOff[s] + (i & 31);
-    const int W = (c.sliceOff[s + 1] - c.sliceOff[s]) >> 5;
-    for (int k = 0; k < W; ++k) {
-      const int e = b + (k << 5);
-      const int j = c.col[e];
-      if (j != i) A[i * n + j] += c.val[e];
+    for (int k = c.rowOff[i]; k < c.rowOff[i + 1]; ++k) {
+      const int j = c.col[k];
+      if (j != i) A[i * n + j] += c.val[k];
     }
   }
   __syncthreads();
@@ -485,18 +585,26 @@ void bicg_init(const LaunchCfg& lc, const BicgArgs& a) {
   k_bicg_init<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
 void bicg_iteration(const LaunchCfg& lc, const BicgArgs& a) {
-  g_launches += 3;
-  k_bicg_p<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  {
+    ProfScope ps(lc, kKfBicgVector, 0.0);
+    k_bicg_p<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
   {
     ProfScope ps(lc, kKfBicgSpmv, lc.ab ? lc.ab->bicg_spmv(a.nc) : 0.0);
     k_bicg_v<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
-  k_bicg_s<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  {
+    ProfScope ps(lc, kKfBicgVector, 0.0);
+    k_bicg_s<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
   {
     ProfScope ps(lc, kKfBicgSpmv, lc.ab ? lc.ab->bicg_spmv(a.nc) : 0.0);
     k_bicg_t<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
-  k_bicg_x<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  {
+    ProfScope ps(lc, kKfBicgVector, 0.0);
+    k_bicg_x<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
 }
 
 void pcg_init(const LaunchCfg& lc, const PcgArgs& a) {
@@ -506,23 +614,73 @@ void pcg_init(const LaunchCfg& lc, const PcgArgs& a) {
 
 static int blocks_for(int n, int cap) { return std::max(1, std::min(cap, (n + kBlock - 1) / kBlock)); }
 
+constexpr int kCoarseLanes = 8;  // lanes per row on the CSR coarse levels
+
 static void vcycle(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
   const int L = amg->nLevels;
-  g_launches += 2 * L - 1;
   // level 0 right-hand side is the PCG residual
-  for (int l = 0; l + 1 < L; ++l) {
-    const AmgLevelDev& f = amg->lv[l];
-    k_amg_down<<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->omega, amg->lv[l + 1].b);
+  {
+    const AmgLevelDev& f = amg->lv[0];
+    ProfScope ps(lc, kKfAmgResid0, 0.0, 2);
+    k_amg_resid<<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+    k_amg_restrict<<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
-  const AmgLevelDev& c = amg->lv[L - 1];
-  k_amg_dense_apply<<<1, 256, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
-  for (int l = L - 2; l >= 0; --l) {
-    const AmgLevelDev& f = amg->lv[l];
-    // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
-    const double* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
-    double* out = (l == 0) ? a.z : f.x2;
-    k_amg_up<<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, out,
-                                                                       l == 0 ? 1 : 0, a);
+  {
+    ProfScope ps(lc, kKfAmgCoarse, 0.0, 3 * L - 6);
+    static const bool lvlTiming = std::getenv("ANB_AMG_LEVEL_TIMING") != nullptr;
+    static double tacc[24][3];
+    static int tcount = 0;
+    cudaEvent_t ev[2];
+    auto tic = [&]() {
+      if (!lvlTiming) return;
+      cudaEventCreate(&ev[0]);
+      cudaEventCreate(&ev[1]);
+      cudaEventRecord(ev[0], lc.stream);
+    };
+    auto toc = [&](int l, int k) {
+      if (!lvlTiming) return;
+      cudaEventRecord(ev[1], lc.stream);
+      cudaEventSynchronize(ev[1]);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      tacc[l][k] += ms;
+      cudaEventDestroy(ev[0]);
+      cudaEventDestroy(ev[1]);
+    };
+    for (int l = 1; l + 1 < L; ++l) {
+      const AmgLevelDev& f = amg->lv[l];
+      tic();
+      k_amg_resid_csr<kCoarseLanes><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
+          a.fl, f, amg->omega);
+      toc(l, 0);
+      tic();
+      k_amg_restrict<<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
+      toc(l, 1);
+    }
+    const AmgLevelDev& c = amg->lv[L - 1];
+    tic();
+    k_amg_dense_apply<<<1, 1024, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
+    toc(L - 1, 0);
+    for (int l = L - 2; l >= 1; --l) {
+      const AmgLevelDev& f = amg->lv[l];
+      // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
+      const double* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
+      tic();
+      k_amg_up_csr<kCoarseLanes><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
+          a.fl, f, e, amg->omega, amg->corr, f.x2);
+      toc(l, 2);
+    }
+    if (lvlTiming && ++tcount % 200 == 0) {
+      for (int l = 1; l < L; ++l)
+        std::fprintf(stderr, "level %d n=%d: resid %.1f us restrict %.1f us up %.1f us\n", l, amg->lv[l].n,
+                     1e3 * tacc[l][0] / tcount, 1e3 * tacc[l][1] / tcount, 1e3 * tacc[l][2] / tcount);
+    }
+  }
+  {
+    const AmgLevelDev& f = amg->lv[0];
+    const double* e = (L == 2) ? amg->lv[1].x : amg->lv[1].x2;
+    ProfScope ps(lc, kKfAmgUp0, 0.0);
+    k_amg_up<<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
   }
 }
 
@@ -530,9 +688,36 @@ void pcg_precondition(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) 
   if (!amg || amg->nLevels < 2) {
     g_launches += 1;
     k_pcg_jacobi<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  } else if (amg->graph) {
+    g_launches += amg->graphKernels;
+    cudaGraphLaunch(amg->graph, lc.stream);
   } else {
     vcycle(lc, a, amg);
   }
+}
+
+// Records one V-cycle into a CUDA graph.  Every pointer and scalar the V-cycle kernels read is
+// fixed for the life of the hierarchy (values change on refresh, addresses do not), so the
+// graph is captured once and replayed for every preconditioner application.
+cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgs& a, AmgDev& amg) {
+  if (amg.graph) {
+    cudaGraphExecDestroy(amg.graph);
+    amg.graph = nullptr;
+  }
+  LaunchCfg quiet = lc;
+  quiet.prof = nullptr;
+  const long long before = g_launches.load();
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(lc.stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  vcycle(quiet, a, &amg);
+  e = cudaStreamEndCapture(lc.stream, &g);
+  amg.graphKernels = (int)(g_launches.load() - before);
+  g_launches -= amg.graphKernels;
+  if (e != cudaSuccess) return e;
+  e = cudaGraphInstantiate(&amg.graph, g, 0);
+  cudaGraphDestroy(g);
+  return e;
 }
 
 void pcg_iteration(const LaunchCfg& lc, const PcgArgs& a, int it, const AmgDev* amg) {
@@ -542,8 +727,10 @@ void pcg_iteration(const LaunchCfg& lc, const PcgArgs& a, int it, const AmgDev* 
     ProfScope ps(lc, kKfPcgSpmv, lc.ab ? lc.ab->pcg_spmv() : 0.0);
     k_pcg_pq<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
   }
-  g_launches += 1;
-  k_pcg_xr<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pNew);
+  {
+    ProfScope ps(lc, kKfPcgUpdate, 0.0);
+    k_pcg_xr<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pNew);
+  }
   pcg_precondition(lc, a, amg);
 }
 
