@@ -89,6 +89,7 @@ struct anb_ctx {
   double *phiStar = nullptr, *phi = nullptr;
   double *bw[8] = {nullptr};  // BiCGSTAB work vectors (3*C each)
   double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pq = nullptr, *pdx = nullptr;
+  double* pwdinv = nullptr;   // omega / pressure diagonal (level-0 smoother)
   double* scal = nullptr;     // device scalars
   int* flags = nullptr;
   double* stats = nullptr;
@@ -347,12 +348,14 @@ void ensure_amg(anb_ctx* c) {
         d.col = c->dm.col;
         d.val = c->pval;
         d.diag = c->pdiag;
+        d.wdinv = c->pwdinv;
       } else {
         d.rowOff = ar.upload(h.rowOff);
         d.col = ar.upload(h.col);
         d.val = ar.alloc<double>(h.rowOff.back());
         d.diag = ar.alloc<double>(h.n);
         d.b = ar.alloc<double>(h.n);
+        d.wdinv = ar.alloc<double>(h.n);
       }
       d.x = ar.alloc<double>(h.n);
       d.x2 = ar.alloc<double>(h.n);
@@ -480,6 +483,8 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   pa.divStar = c->divStar;
   pa.b = c->pb;
   pa.pc = c->Pc;
+  pa.wdinv = c->pwdinv;
+  pa.omega = c->amg.omega;
   launch_pressure_rc(c->lc, c->dm, pa);
   const int every = std::max(p.p_amg_rebuild_every, 1);
   if (!c->amgBuilt || c->outerStep == 1 || ((c->outerStep - 1) % every) == 0) ensure_amg(c);
@@ -760,6 +765,9 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     c->pp1 = A.alloc<double>(C);
     c->pq = A.alloc<double>(C);
     c->pdx = A.alloc<double>(C);
+    c->pwdinv = A.alloc<double>(C);
+    if (const char* s = std::getenv("ANB_AMG_OMEGA")) c->amg.omega = std::atof(s);
+    if (const char* s = std::getenv("ANB_AMG_CORR")) c->amg.corr = std::atof(s);
     c->scal = A.alloc<double>(64);
     c->flags = A.alloc<int>(32);
     c->stats = A.alloc<double>(16);
@@ -1043,6 +1051,8 @@ int anb_debug_pressure(anb_ctx* c, const double* u, const double* v, const doubl
     pa.divStar = c->divStar;
     pa.b = c->pb;
     pa.pc = c->Pc;
+    pa.wdinv = c->pwdinv;
+    pa.omega = c->amg.omega;
     launch_pressure_rc(c->lc, c->dm, pa);
     CK(cudaGetLastError());
     double* d1[1] = {diag};

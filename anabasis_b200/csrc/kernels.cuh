@@ -121,6 +121,8 @@ struct PresArgs {
   double* divStar;
   double* b;          // first pressure right-hand side, -divStar
   double* pc;         // zeroed p'
+  double* wdinv;      // optional: omega / diag for the AMG smoother
+  double omega;
 };
 void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgs& a);
 
@@ -208,14 +210,19 @@ struct AmgLevelDev {
   int nEntNext;        // next level's SELL storage entries
   // work vectors
   double *b, *x, *x2;
+  double* wdinv;       // omega / diag (Jacobi smoother)
 };
 struct AmgDev {
   int nLevels = 0;
   AmgLevelDev lv[24];
   double* dense = nullptr;   // coarsest inverse, n_L^2
   int nDense = 0;
-  double omega = 0.6667;     // Jacobi weight
-  double corr = 1.0;         // coarse-correction scaling
+  // Jacobi weight and coarse-correction scaling of the symmetric V(1,1)-cycle.  Piecewise-constant
+  // prolongation under-estimates smooth error, and scaling the coarse correction (over-correction)
+  // compensates; any positive scaling keeps the V-cycle SPD.  0.9 / 1.6 minimised the PCG
+  // iterations on the jittered obstacle channel (105 -> 66 per outer step at 970k cells).
+  double omega = 0.9;
+  double corr = 1.6;
   cudaGraphExec_t graph = nullptr;  // captured V-cycle (see amg_capture_graph)
   int graphKernels = 0;
 };

@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgs a) {
       a.phiStar[nI + bf] = phi;
     }
     a.diag[r] = pd;
+    if (a.wdinv) a.wdinv[r] = a.omega / pd;  // level-0 smoother weight, always from the current matrix
     a.divStar[r] = div;
     a.b[r] = -div;
     a.pc[r] = 0.0;

@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
     const double di = __ldg(&f.diag[i]);
     const double bi = __ldg(&f.b[i]);
-    const double xi = omega * bi / di;
+    const double xi = __ldg(&f.wdinv[i]) * bi;
     double ax = di * xi;
     const int s = i >> 5;
     const int b = __ldg(&f.sliceOff[s]) + (i & 31);
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
     for (int k = 0; k < W; ++k) {
       const int e = b + (k << 5);
       const int j = __ldg(&f.col[e]);
-      ax += __ldg(&f.val[e]) * (omega * __ldg(&f.b[j]) / __ldg(&f.diag[j]));
+      ax += __ldg(&f.val[e]) * (__ldg(&f.wdinv[j]) * __ldg(&f.b[j]));
     }
     f.x[i] = xi;
     f.x2[i] = bi - ax;
@@ -407,13 +407,13 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLe
       const int k1 = __ldg(&f.rowOff[i + 1]);
       for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
         const int j = __ldg(&f.col[k]);
-        acc += __ldg(&f.val[k]) * (omega * __ldg(&f.b[j]) / __ldg(&f.diag[j]));
+        acc += __ldg(&f.val[k]) * (__ldg(&f.wdinv[j]) * __ldg(&f.b[j]));
       }
     }
     acc = group_sum<G>(acc);
     if (i < f.n && sub == 0) {
       const double di = __ldg(&f.diag[i]), bi = __ldg(&f.b[i]);
-      const double xi = omega * bi / di;
+      const double xi = __ldg(&f.wdinv[i]) * bi;
       f.x[i] = xi;
       f.x2[i] = bi - di * xi - acc;
     }
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevel
     if (i < f.n && sub == 0) {
       const double di = __ldg(&f.diag[i]);
       const double xi = __ldg(&f.x[i]) + corr * __ldg(&e[__ldg(&f.agg[i])]);
-      out[i] = xi + omega * (__ldg(&f.b[i]) - di * xi - acc) / di;
+      out[i] = xi + __ldg(&f.wdinv[i]) * (__ldg(&f.b[i]) - di * xi - acc);
     }
   }
 }
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
       const int j = __ldg(&f.col[ee]);
       ax += __ldg(&f.val[ee]) * (__ldg(&f.x[j]) + corr * __ldg(&e[__ldg(&f.agg[j])]));
     }
-    const double xn = xi + omega * (__ldg(&f.b[i]) - ax) / di;
+    const double xn = xi + __ldg(&f.wdinv[i]) * (__ldg(&f.b[i]) - ax);
     out[i] = xn;
     if (finest) acc[0] += f.b[i] * xn;
   }
@@ -508,7 +508,8 @@ __global__ void k_amg_dense_apply(const int* done, int n, const double* inv, con
 }
 
 // Galerkin values of the next level: one gather list per coarse storage entry.
-__global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDev f, double* valNext, double* diagNext) {
+__global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDev f, double* valNext, double* diagNext,
+                                                         double* wdinvNext, double omega) {
   const int nT = f.nEntNext + f.nc;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nT; t += gridDim.x * blockDim.x) {
     double s = 0.0;
@@ -516,8 +517,12 @@ __global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDev f, double* 
       const int idx = f.gIdx[k];
       s += idx >= 0 ? f.val[idx] : f.diag[-1 - idx];
     }
-    if (t < f.nEntNext) valNext[t] = s;
-    else diagNext[t - f.nEntNext] = s;
+    if (t < f.nEntNext) {
+      valNext[t] = s;
+    } else {
+      diagNext[t - f.nEntNext] = s;
+      wdinvNext[t - f.nEntNext] = omega / s;
+    }
   }
 }
 
@@ -739,7 +744,8 @@ void amg_refresh(const LaunchCfg& lc, AmgDev& amg) {
     AmgLevelDev& f = amg.lv[l];
     AmgLevelDev& c = amg.lv[l + 1];
     g_launches += 1;
-    k_amg_galerkin<<<blocks_for(f.nEntNext + f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(f, c.val, c.diag);
+    k_amg_galerkin<<<blocks_for(f.nEntNext + f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(f, c.val, c.diag,
+                                                                                          c.wdinv, amg.omega);
   }
   const AmgLevelDev& c = amg.lv[amg.nLevels - 1];
   const size_t smem = sizeof(double) * (size_t)c.n * c.n;
