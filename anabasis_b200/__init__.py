@@ -73,6 +73,7 @@ SIGNATURES = {
     "anb_get_state": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "anb_simple_iterate": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.POINTER(IterStats), _ip]),
     "anb_patch_force": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
+    "anb_patch_force_nalloc": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
     "anb_profile_select": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "anb_profile_read": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_longlong), _dp, _dp]),
     "anb_launch_count": (ct.c_longlong, []),

@@ -11,6 +11,7 @@
 
 #include "../../include/anb.h"
 #include "amg_setup.hpp"
+#include "context_access.hpp"
 #include "host_mesh.hpp"
 #include "kernels.cuh"
 #include "layout.hpp"
@@ -1089,3 +1090,26 @@ int anb_debug_pressure_solve(anb_ctx* c, const double* b, double* x, int* iters,
 }
 
 }  // extern "C"
+
+namespace anb {
+
+bool context_force_view(const anb_ctx* c, int patch, ForceView* v) {
+  if (!c || patch < 0 || patch >= (int)c->hm.patches.size()) return false;
+  v->dm = c->dm;
+  v->b0 = c->hm.patches[patch].start - c->nI;
+  v->b1 = v->b0 + c->hm.patches[patch].nFaces;
+  v->mu = c->prm.mu;
+  v->bA = c->dBA;
+  v->bN = c->dBN;
+  v->U = c->U;
+  v->P = c->P;
+  v->stream = c->stream;
+  v->device = c->prm.device;
+  return true;
+}
+
+void context_set_error(anb_ctx* c, const char* msg) {
+  if (c) c->err = msg;
+}
+
+}  // namespace anb

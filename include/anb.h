@@ -129,6 +129,18 @@ int anb_simple_iterate(anb_ctx* ctx, int nsteps, double tol_mass, double tol_vel
  * patch is the 0-based patch index in input order. */
 int anb_patch_force(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* out);
 
+/* Same integral as anb_patch_force, for callers that cannot allocate device memory when they
+ * ask for it (an application that owns the whole GPU through its own pool, code running while
+ * another component records a CUDA graph, a plugin with a fixed memory budget).  No counterpart
+ * in the reference.  The call allocates nothing: its scratch (block partial sums, result,
+ * arrival counter) is one file-scope __device__ array of 131,216 bytes that every GPU loading
+ * the library keeps until the process exits.  Limit: patches of at most 262,144 faces
+ * (ANB_ERR_INVALID beyond).  The first call on a device looks up the array's device address
+ * and clears its counter; make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU (several threads or contexts on one device at once)
+ * race and must be serialised by the caller. */
+int anb_patch_force_nalloc(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* out);
+
 /* ---- measurement (no counterpart in the reference; used by the benchmark) ------------------
  * Kernel families for anb_profile_select: every launch of the selected family is bracketed by
  * CUDA events on the context's stream and its algorithmic (compulsory) bytes are accumulated. */
