@@ -315,6 +315,17 @@ class Solver:
             pass
 
 
+def expand_case_args(argv: list[str]) -> list[str]:
+    """`-case-config` expansion of the front end (raises AnbError with the reference's message)."""
+    arr = (ct.c_char_p * len(argv))(*[a.encode() for a in argv])
+    out = ct.create_string_buffer(1 << 16)
+    err = ct.create_string_buffer(4096)
+    n = lib().anb_expand_case_args(len(argv), arr, out, 1 << 16, err, 4096)
+    if n < 0:
+        raise AnbError(ANB_ERR_INVALID, err.value.decode())
+    return [s.decode() for s in out.raw.split(b"\0")[:n]]
+
+
 def build(force: bool = False) -> Path:
     from .build import build as _build
     return _build(force=force)

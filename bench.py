@@ -90,6 +90,22 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(sm)}
 
 
+def max_over_ranks(values: list[float], dist=None, device: str = "cpu") -> list[float]:
+    """Element-wise maximum over all ranks (the timed region is the slowest rank's)."""
+    if dist is None:
+        return list(values)
+    import torch
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def replica_throughput(world: int, cells: int, steps: int, t_max: float) -> float:
+    """Whole-job cell-iterations/s of `world` independent replicas (weak scaling)."""
+    return world * cells * steps / t_max
+
+
 def make_case():
     from tests.cases import channel, initial_state
 
@@ -140,20 +156,15 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         s.iterate(1)
         g = s.get_state(with_phi=False)
     e2e_wall = time.perf_counter() - te
-    t_max = dev_seconds
+    t_max, e2e_wall = max_over_ranks([dev_seconds, e2e_wall], dist, f"cuda:{local_rank}")
     if dist:
-        import torch
-
-        t = torch.tensor([dev_seconds, e2e_wall], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max, e2e_wall = float(t[0]), float(t[1])
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return None
     peak, peak_kind = measured_peaks()
     achieved = (byts[0] / secs[0] / 1e9) if secs[0] > 0 else None
-    value = world * C * args.steps / t_max
+    value = replica_throughput(world, C, args.steps, t_max)
     cpu = cpu_baseline(m, bc, (u0, v0, w0, p0)) if world == 1 and not args.no_cpu else None
     out = {
         "metric": "SIMPLE cell-iters/s",
@@ -172,7 +183,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                                "2 non-orthogonal correctors, inner tol 1e-10",
                    "cells": C, "internal_faces": m.n_internal, "parallelism": f"replicas{world}",
                    "l2": "working set > L2 (no flush needed)", "wall_seconds_timed": wall},
-        "e2e": {"value": world * C * e2e_steps / e2e_wall, "unit": "cell-iters/s",
+        "e2e": {"value": replica_throughput(world, C, e2e_steps, e2e_wall), "unit": "cell-iters/s",
                 "h2d_bytes_per_step": 4 * 8 * C, "d2h_bytes_per_step": 4 * 8 * C},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": FAMILY_NAMES[KERNEL_FAMILY], "achieved": achieved,

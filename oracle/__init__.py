@@ -53,6 +53,8 @@ def lib() -> ct.CDLL:
         L.orc_momentum.argtypes = [ct.c_void_p, ct.c_double, ct.c_double, ct.c_double, _dp, _dp, _dp, _dp, _dp, _dp,
                                    _dp, _dp, _dp]
         L.orc_pressure.argtypes = [ct.c_void_p, ct.c_double, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.orc_nonorth.argtypes = [ct.c_void_p, _dp, _dp, _dp, _dp]
+        L.orc_flux_correct.argtypes = [ct.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.orc_simple_run.restype = ct.c_int
         L.orc_simple_run.argtypes = [ct.c_void_p, ct.POINTER(OrcParams), ct.c_int, _dp, _dp, _dp, _dp, _dp,
                                      ct.POINTER(OrcStats)]
@@ -123,6 +125,20 @@ class Oracle:
         lib().orc_pressure(self._h, rho, *map(_d, arrs), _d(o["diag"]), _d(o["a_pn"]), _d(o["phi_star"]),
                            _d(o["div_star"]))
         return o
+
+    def nonorth(self, rau, grad) -> tuple[np.ndarray, np.ndarray]:
+        phi = np.zeros(self.n_faces)
+        div = np.zeros(self.n_cells)
+        g = np.ascontiguousarray(np.asarray(grad, np.float64).reshape(-1))
+        lib().orc_nonorth(self._h, _d(np.ascontiguousarray(rau, np.float64)), _d(g), _d(phi), _d(div))
+        return phi, div
+
+    def flux_correct(self, rau, phi_star, pcorr, grad) -> np.ndarray:
+        out = np.zeros(self.n_faces)
+        g = np.ascontiguousarray(np.asarray(grad, np.float64).reshape(-1))
+        a = [np.ascontiguousarray(x, np.float64) for x in (rau, phi_star, pcorr)]
+        lib().orc_flux_correct(self._h, *map(_d, a), _d(g), _d(out))
+        return out
 
     def run(self, params: OrcParams, nsteps: int, u, v, w, p) -> tuple[dict, list]:
         st = (OrcStats * max(nsteps, 1))()

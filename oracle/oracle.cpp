@@ -781,6 +781,35 @@ void orc_pressure(const orc_mesh* mc, double rho, const double* u, const double*
   if (div_star) std::memcpy(div_star, dv.data(), sizeof(double) * m.nCells);
 }
 
+void orc_nonorth(const orc_mesh* m, const double* rau, const double* g, double* phi_no, double* div_no) {
+  const int n = m->nCells;
+  G3 gg(n);
+  for (int c = 0; c < n; ++c) {
+    gg.x[c] = g[c];
+    gg.y[c] = g[n + c];
+    gg.z[c] = g[2 * n + c];
+  }
+  std::vector<double> a(m->nFaces), b(n);
+  nonorth(*m, rau, gg, a, b);
+  std::memcpy(phi_no, a.data(), sizeof(double) * m->nFaces);
+  std::memcpy(div_no, b.data(), sizeof(double) * n);
+}
+
+void orc_flux_correct(const orc_mesh* m, const double* rau, const double* phi_star, const double* pcorr,
+                      const double* g, double* phi) {
+  const int n = m->nCells;
+  G3 gg(n);
+  for (int c = 0; c < n; ++c) {
+    gg.x[c] = g[c];
+    gg.y[c] = g[n + c];
+    gg.z[c] = g[2 * n + c];
+  }
+  std::vector<double> no(m->nFaces), dno(n), ps(phi_star, phi_star + m->nFaces), out(m->nFaces);
+  nonorth(*m, rau, gg, no, dno);
+  flux_correct(*m, rau, ps, pcorr, no, out);
+  std::memcpy(phi, out.data(), sizeof(double) * m->nFaces);
+}
+
 // SIMPLE loop, GSV1:3350-3634.
 int orc_simple_run(orc_mesh* mp, const orc_params* prm, int nsteps, double* uIO, double* vIO, double* wIO,
                    double* pIO, double* phiOut, orc_stats* stats) {

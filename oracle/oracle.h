@@ -65,6 +65,12 @@ void orc_pressure(const orc_mesh* m, double rho, const double* u, const double* 
                   const double* p, const double* rau, double* diag, double* a_pn, double* phi_star,
                   double* div_star);
 
+/* kernel_pressure_nonorth_flux_and_divergence (GSV1:1538-1593) for p' gradient g (3 x nCells SoA),
+ * and kernel_correct_face_fluxes_simple_nonorth (GSV1:1615-1658) on top of it */
+void orc_nonorth(const orc_mesh* m, const double* rau, const double* g, double* phi_no, double* div_no);
+void orc_flux_correct(const orc_mesh* m, const double* rau, const double* phi_star, const double* pcorr,
+                      const double* g, double* phi);
+
 /* nsteps SIMPLE iterations (GSV1:3388-3634).  u,v,w,p in/out, phi out (nFaces).  stats may be
  * NULL (else nsteps entries).  Returns executed steps (early stop on convergence). */
 int orc_simple_run(orc_mesh* m, const orc_params* prm, int nsteps, double* u, double* v, double* w,
