@@ -632,53 +632,20 @@ static void vcycle(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
   }
   {
     ProfScope ps(lc, kKfAmgCoarse, 0.0, 3 * L - 6);
-    static const bool lvlTiming = std::getenv("ANB_AMG_LEVEL_TIMING") != nullptr;
-    static double tacc[24][3];
-    static int tcount = 0;
-    cudaEvent_t ev[2];
-    auto tic = [&]() {
-      if (!lvlTiming) return;
-      cudaEventCreate(&ev[0]);
-      cudaEventCreate(&ev[1]);
-      cudaEventRecord(ev[0], lc.stream);
-    };
-    auto toc = [&](int l, int k) {
-      if (!lvlTiming) return;
-      cudaEventRecord(ev[1], lc.stream);
-      cudaEventSynchronize(ev[1]);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, ev[0], ev[1]);
-      tacc[l][k] += ms;
-      cudaEventDestroy(ev[0]);
-      cudaEventDestroy(ev[1]);
-    };
     for (int l = 1; l + 1 < L; ++l) {
       const AmgLevelDev& f = amg->lv[l];
-      tic();
       k_amg_resid_csr<kCoarseLanes><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, amg->omega);
-      toc(l, 0);
-      tic();
       k_amg_restrict<<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
-      toc(l, 1);
     }
     const AmgLevelDev& c = amg->lv[L - 1];
-    tic();
     k_amg_dense_apply<<<1, 1024, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
-    toc(L - 1, 0);
     for (int l = L - 2; l >= 1; --l) {
       const AmgLevelDev& f = amg->lv[l];
       // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
       const double* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
-      tic();
       k_amg_up_csr<kCoarseLanes><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, e, amg->omega, amg->corr, f.x2);
-      toc(l, 2);
-    }
-    if (lvlTiming && ++tcount % 200 == 0) {
-      for (int l = 1; l < L; ++l)
-        std::fprintf(stderr, "level %d n=%d: resid %.1f us restrict %.1f us up %.1f us\n", l, amg->lv[l].n,
-                     1e3 * tacc[l][0] / tcount, 1e3 * tacc[l][1] / tcount, 1e3 * tacc[l][2] / tcount);
     }
   }
   {

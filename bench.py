@@ -34,6 +34,11 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = dict(nx=200, ny=70, nz=70, jitter=0.15, seed=0, obstacle=True)
 PARAMS = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3, n_nonorth_corr=2)
 KERNEL_FAMILY = 7  # ANB_KF_PCG_SPMV: the dominant kernel of the step (see profiles/)
+# DRAM bytes (read + write) per k_pcg_pq launch on this workload: mean of 3 launches of
+#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
+#       -k k_pcg_pq -s 30 -c 3 python bench.py --steps 2 --warmup 3 --no-cpu
+# (93.10 MB read + 3.44 MB write; profiles/k_pcg_pq_obstacle1m.md)
+PCG_SPMV_TRAFFIC_BYTES = 96.53e6
 FAMILY_NAMES = {1: "k_lsq_grad", 2: "k_momentum", 3: "k_pressure_rc", 4: "k_nonorth_rhs", 5: "k_flux_final",
                 6: "k_bicg_v/k_bicg_t", 7: "k_pcg_pq"}
 
@@ -49,7 +54,8 @@ def measured_peaks() -> tuple[float, str]:
 
 
 class ClockSampler:
-    """nvidia-smi SM clock / throttle-reason samples every 200 ms during the timed region."""
+    """SM clock / throttle-reason samples during the timed region: NVML reads every 20 ms (read-only
+    queries), else nvidia-smi every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -59,18 +65,52 @@ class ClockSampler:
         self.device = device
         self.rows: list[list[str]] = []
         self._stop = threading.Event()
+        self._nvml = self._nvml_handle()
         self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _nvml_handle(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            bus = None
+            try:
+                import torch
+
+                if torch.cuda.is_available():
+                    p = torch.cuda.get_device_properties(self.device)
+                    bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            except Exception:
+                bus = None
+            h = (pynvml.nvmlDeviceGetHandleByPciBusId(bus) if bus else pynvml.nvmlDeviceGetHandleByIndex(self.device))
+            return pynvml, h
+        except Exception:
+            return None
+
+    def _sample_nvml(self):
+        nv, h = self._nvml
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        self.rows.append([str(self.device), str(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                          str(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                          str(nv.nvmlDeviceGetPowerUsage(h) / 1000.0), hex(r)]
+                         + ["Active" if r & b else "Not Active" for b in bits])
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.rows.append([x.strip() for x in line.split(",")])
+                if self._nvml is not None:
+                    self._sample_nvml()
+                else:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5)
+                    for line in out.stdout.strip().splitlines():
+                        self.rows.append([x.strip() for x in line.split(",")])
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.02 if self._nvml is not None else 0.2)
 
     def __enter__(self):
         self._t.start()
@@ -189,7 +229,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "roofline": {"bound": "hbm", "kernel": FAMILY_NAMES[KERNEL_FAMILY], "achieved": achieved,
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "launches": int(n_l.value), "traffic": None},
+                     "launches": int(n_l.value), "algorithmic_bytes": byts[0] / max(int(n_l.value), 1),
+                     "traffic": PCG_SPMV_TRAFFIC_BYTES if KERNEL_FAMILY == 7 else None},
         "inner": {"bicgstab_last": [st[-1]["its_u"], st[-1]["its_v"], st[-1]["its_w"]],
                   "pcg_total_last": st[-1]["its_p_total"], "mass_res_last": st[-1]["mass_res"]},
         "clocks": clk.summary(),
