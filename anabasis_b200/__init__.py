@@ -60,6 +60,11 @@ class ForceReport(ct.Structure):
                 ("max_wall_distance", ct.c_double), ("max_ut", ct.c_double), ("max_shear_mag", ct.c_double)]
 
 
+class SolveInfo(ct.Structure):
+    _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("outer", ct.c_int),
+                ("final_res_norm", ct.c_double), ("final_rel_res", ct.c_double)]
+
+
 # exported symbols and their signatures (restype, argtypes); checked against include/*.h by tests
 SIGNATURES = {
     "anb_default_params": (None, [ct.POINTER(Params)]),
@@ -74,6 +79,11 @@ SIGNATURES = {
     "anb_simple_iterate": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.POINTER(IterStats), _ip]),
     "anb_patch_force": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
     "anb_patch_force_nalloc": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
+    "anb_scalar_elliptic_solve": (ct.c_int, [ct.c_void_p, _dp, _dp, _ip, _dp, ct.c_int, ct.c_int, ct.c_int, ct.c_int,
+                                             ct.c_double, ct.c_double, ct.c_double, ct.c_int, _dp,
+                                             ct.POINTER(SolveInfo)]),
+    "anb_scalar_transport_solve": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _ip, _dp, ct.c_int, ct.c_int, ct.c_int,
+                                              ct.c_double, ct.c_double, ct.c_int, _dp, _dp, ct.POINTER(SolveInfo)]),
     "anb_profile_select": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "anb_profile_read": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_longlong), _dp, _dp]),
     "anb_launch_count": (ct.c_longlong, []),
@@ -257,6 +267,37 @@ class Solver:
         o["phi"] = np.zeros(F) if with_phi else None
         self._check(lib().anb_get_state(self._h, _d(o["u"]), _d(o["v"]), _d(o["w"]), _d(o["p"]), _d(o["phi"])))
         return o
+
+    def scalar_elliptic_solve(self, cell_source, bc_type, bc_value, gamma_face=None, laplacian_nonorth=True,
+                              nonorth_corr=2, use_reference_cell=False, reference_cell=0, reference_value=0.0,
+                              abs_tol=1e-12, rel_tol=0.0, max_iter=4000) -> tuple[np.ndarray, dict]:
+        """anb_scalar_elliptic_solve: face arrays nFaces long (input order), cell arrays nCells."""
+        phi = np.zeros(self.n_cells)
+        info = SolveInfo()
+        g = None if gamma_face is None else np.ascontiguousarray(gamma_face, np.float64)
+        src = np.ascontiguousarray(cell_source, np.float64)
+        bt = np.ascontiguousarray(bc_type, np.int32)
+        bv = np.ascontiguousarray(bc_value, np.float64)
+        self._check(lib().anb_scalar_elliptic_solve(self._h, _d(g), _d(src), _i(bt), _d(bv), int(laplacian_nonorth),
+                                                    nonorth_corr, int(use_reference_cell), reference_cell,
+                                                    reference_value, abs_tol, rel_tol, max_iter, _d(phi),
+                                                    ct.byref(info)), ok=(ANB_OK, ANB_NOT_CONVERGED))
+        return phi, dict((f, getattr(info, f)) for f, _ in SolveInfo._fields_)
+
+    def scalar_transport_solve(self, gamma_face, su, bc_type, bc_value, face_flux=None, sp=None, upwind=False,
+                               diffusion_nonorth=True, nonorth_corr=2, abs_tol=1e-10, rel_tol=0.0, max_iter=4000,
+                               x0=None) -> tuple[np.ndarray, dict]:
+        """anb_scalar_transport_solve: face arrays nFaces long (input order), cell arrays nCells."""
+        phi = np.zeros(self.n_cells)
+        info = SolveInfo()
+        arr = lambda a, t=np.float64: None if a is None else np.ascontiguousarray(a, t)  # noqa: E731
+        g, s_u, s_p, fl, x = arr(gamma_face), arr(su), arr(sp), arr(face_flux), arr(x0)
+        bt, bv = arr(bc_type, np.int32), arr(bc_value)
+        self._check(lib().anb_scalar_transport_solve(self._h, _d(fl), _d(g), _d(s_u), _d(s_p), _i(bt), _d(bv),
+                                                     int(upwind), int(diffusion_nonorth), nonorth_corr, abs_tol,
+                                                     rel_tol, max_iter, _d(x), _d(phi), ct.byref(info)),
+                    ok=(ANB_OK, ANB_NOT_CONVERGED))
+        return phi, dict((f, getattr(info, f)) for f, _ in SolveInfo._fields_)
 
     def iterate(self, nsteps: int, tol_mass=-1.0, tol_vel=-1.0) -> tuple[int, list]:
         st = (IterStats * max(nsteps, 1))()

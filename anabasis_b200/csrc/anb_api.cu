@@ -111,6 +111,11 @@ struct anb_ctx {
   // measurement
   Prof prof;
   AlgoBytes ab;
+  // scalar-library solves (allocated on first use)
+  DevArena scalarArena;
+  double *sMinv = nullptr, *sBcVal = nullptr, *sGamma = nullptr, *sFlux = nullptr, *sSrc = nullptr,
+         *sSp = nullptr, *sPhi = nullptr, *sGrad = nullptr;
+  uint8_t* sBcType = nullptr;
 };
 
 namespace {
@@ -942,6 +947,257 @@ int anb_patch_force(anb_ctx* c, int patch, int sign, anb_force_report* out) {
     out->max_ut = h[13];
     out->max_shear_mag = h[14];
     return ANB_OK;
+  });
+}
+
+// ---- scalar libraries -------------------------------------------------------------------------
+namespace {
+
+void release_amg(anb_ctx* c) {
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
+  c->amg.graph = nullptr;
+  c->amg.graphKernels = 0;
+  c->amg.nLevels = 0;
+  c->amg.dense = nullptr;
+  c->amgArena.release();
+  c->amgHost.clear();
+  c->amgBuilt = false;
+}
+
+void ensure_scalar_buffers(anb_ctx* c) {
+  if (c->sPhi) return;
+  DevArena& A = c->scalarArena;
+  const int C = c->C, nF = c->nI + c->nB;
+  c->sMinv = A.alloc<double>((size_t)6 * C);
+  c->sBcType = A.alloc<uint8_t>(c->nB);
+  c->sBcVal = A.alloc<double>(c->nB);
+  c->sGamma = A.alloc<double>(nF);
+  c->sFlux = A.alloc<double>(nF);
+  c->sSrc = A.alloc<double>(C);
+  c->sSp = A.alloc<double>(C);
+  c->sPhi = A.alloc<double>(C);
+  c->sGrad = A.alloc<double>((size_t)3 * C);
+}
+
+// Face array in input order/orientation -> device (layout order; fluxes change sign on flipped
+// internal faces).  src == nullptr uploads `fill`.
+void upload_faces(anb_ctx* c, const double* src, double* dst, bool orientSign, double fill) {
+  const int nF = c->nI + c->nB;
+  std::vector<double> h(nF, fill);
+  if (src) {
+    for (int fi = 0; fi < c->nI; ++fi) {
+      const double v = src[c->L.fOrig[fi]];
+      h[fi] = (orientSign && c->L.fFlip[fi]) ? -v : v;
+    }
+    for (int b = 0; b < c->nB; ++b) h[c->nI + b] = src[c->nI + b];
+  }
+  CK(cudaMemcpyAsync(dst, h.data(), nF * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+void upload_cells1(anb_ctx* c, const double* src, double* dst, double fill) {
+  if (src) {
+    const double* s[1] = {src};
+    upload_cells(c, s, dst, 1);
+  } else {
+    std::vector<double> h(c->C, fill);
+    CK(cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+}
+
+// Boundary types/values (nFaces arrays, boundary entries read) -> device, LSQ inverse for them.
+void upload_scalar_bc(anb_ctx* c, const int* type, const double* value, int maxType) {
+  std::vector<uint8_t> t(c->nB), dir(c->nB);
+  std::vector<double> v(c->nB);
+  for (int b = 0; b < c->nB; ++b) {
+    const int ty = type[c->nI + b];
+    if (ty < 0 || ty > maxType)
+      throw AnbError(ANB_ERR_INVALID, "invalid scalar boundary type " + std::to_string(ty) + " at face " +
+                                          std::to_string(c->nI + b));
+    t[b] = (uint8_t)ty;
+    dir[b] = ty == ANB_SCALAR_DIRICHLET;
+    v[b] = value[c->nI + b];
+  }
+  const std::vector<double> minv = scalar_lsq_minv(c->hm, c->L, dir);
+  CK(cudaMemcpyAsync(c->sBcType, t.data(), t.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->sBcVal, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->sMinv, minv.data(), minv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+}
+
+ScalarArgs scalar_args(anb_ctx* c) {
+  ScalarArgs a{};
+  a.phi = c->sPhi;
+  a.minv = c->sMinv;
+  a.bcType = c->sBcType;
+  a.bcVal = c->sBcVal;
+  a.bA = c->dBA;
+  a.bN = c->dBN;
+  a.gammaF = c->sGamma;
+  a.src = c->sSrc;
+  a.grad = c->sGrad;
+  a.g = c->sGrad;
+  a.refCell = -1;
+  a.omega = c->amg.omega;
+  return a;
+}
+
+void download_cells1(anb_ctx* c, const double* src, double* dst) {
+  double* d[1] = {dst};
+  download_cells(c, src, d, 1);
+}
+
+}  // namespace
+
+int anb_scalar_elliptic_solve(anb_ctx* c, const double* gammaFace, const double* source, const int* bcType,
+                              const double* bcValue, int nonorth, int nNonOrthCorr, int useRef, int refCell,
+                              double refValue, double absTol, double relTol, int maxIter, double* phi,
+                              anb_solve_info* info) {
+  if (!c || !source || !bcType || !bcValue || !phi) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    CK(cudaSetDevice(c->prm.device));
+    if (info) std::memset(info, 0, sizeof(*info));
+    bool anyDirichlet = false;
+    for (int b = 0; b < c->nB && !anyDirichlet; ++b) anyDirichlet = bcType[c->nI + b] == ANB_SCALAR_DIRICHLET;
+    if (!anyDirichlet && !useRef)
+      throw AnbError(ANB_ERR_INVALID, "Pure-Neumann scalar elliptic problem needs useReferenceCell=true.");
+    if (useRef && (refCell < 0 || refCell >= c->C)) throw AnbError(ANB_ERR_INVALID, "Invalid reference cell");
+    ensure_scalar_buffers(c);
+    upload_scalar_bc(c, bcType, bcValue, ANB_SCALAR_NEUMANN);
+    upload_faces(c, gammaFace, c->sGamma, false, 1.0);
+    upload_cells1(c, source, c->sSrc, 0.0);
+    CK(cudaMemsetAsync(c->sPhi, 0, sizeof(double) * c->C, c->stream));
+    CK(cudaMemsetAsync(c->sGrad, 0, sizeof(double) * 3 * c->C, c->stream));
+    ScalarArgs a = scalar_args(c);
+    a.transport = 0;
+    a.nonorth = nonorth != 0;
+    a.refCell = useRef ? c->L.old2new[refCell] : -1;
+    a.refValue = refValue;
+    a.val = c->pval;
+    a.diag = c->pdiag;
+    a.rhs = c->pb;
+    a.wdinv = c->pwdinv;
+    const int nOuter = nonorth ? std::max(nNonOrthCorr, 0) + 1 : 1;
+    // the matrix stays the same across passes (only the non-orthogonal rhs changes): one AMG set-up
+    release_amg(c);
+    const double saveTol = c->prm.p_tol;
+    const int saveMaxit = c->prm.p_maxit;
+    c->prm.p_tol = absTol;
+    c->prm.p_maxit = maxIter;
+    int its = 0;
+    bool conv = true, allConv = true;
+    try {
+      for (int outer = 0; outer < nOuter; ++outer) {
+        if (a.nonorth) launch_scalar_grad(c->lc, c->dm, a);
+        launch_scalar_assemble(c->lc, c->dm, a);
+        if (outer == 0) ensure_amg(c);
+        CK(cudaMemsetAsync(c->sPhi, 0, sizeof(double) * c->C, c->stream));
+        solve_pressure(c, c->pb, c->sPhi, relTol, &its, &conv);
+        allConv = allConv && conv;
+      }
+    } catch (...) {
+      c->prm.p_tol = saveTol;
+      c->prm.p_maxit = saveMaxit;
+      release_amg(c);
+      throw;
+    }
+    c->prm.p_tol = saveTol;
+    c->prm.p_maxit = saveMaxit;
+    double sc[8];
+    CK(cudaMemcpyAsync(sc, c->scal + kScalPcg, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    release_amg(c);  // the SIMPLE path rebuilds its own hierarchy
+    download_cells1(c, c->sPhi, phi);
+    if (info) {
+      info->iterations = its;
+      info->converged = allConv ? 1 : 0;
+      info->outer = nOuter;
+      info->final_res_norm = std::sqrt(std::max(sc[4], 0.0));
+      // eps = max(atol, rtol |b|) is not |b|; recompute |b| on the host from the assembled rhs
+      std::vector<double> hb(c->C);
+      CK(cudaMemcpy(hb.data(), c->pb, sizeof(double) * c->C, cudaMemcpyDeviceToHost));
+      double bn = 0.0;
+      for (double x : hb) bn += x * x;
+      info->final_rel_res = bn > 0.0 ? info->final_res_norm / std::sqrt(bn) : 0.0;
+    }
+    return allConv ? ANB_OK : ANB_NOT_CONVERGED;
+  });
+}
+
+int anb_scalar_transport_solve(anb_ctx* c, const double* flux, const double* gammaFace, const double* su,
+                               const double* sp, const int* bcType, const double* bcValue, int convection,
+                               int nonorth, int nNonOrthCorr, double absTol, double relTol, int maxIter,
+                               const double* x0, double* phi, anb_solve_info* info) {
+  if (!c || !gammaFace || !su || !bcType || !bcValue || !phi) return ANB_ERR_INVALID;
+  if (convection != ANB_CONVECTION_CENTRAL && convection != ANB_CONVECTION_UPWIND) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    CK(cudaSetDevice(c->prm.device));
+    if (info) std::memset(info, 0, sizeof(*info));
+    ensure_scalar_buffers(c);
+    upload_scalar_bc(c, bcType, bcValue, ANB_SCALAR_ZERO_GRADIENT);
+    upload_faces(c, gammaFace, c->sGamma, false, 0.0);
+    if (flux) upload_faces(c, flux, c->sFlux, true, 0.0);
+    upload_cells1(c, su, c->sSrc, 0.0);
+    upload_cells1(c, sp, c->sSp, 0.0);
+    upload_cells1(c, x0, c->sPhi, 0.0);
+    CK(cudaMemsetAsync(c->sGrad, 0, sizeof(double) * 3 * c->C, c->stream));
+    ScalarArgs a = scalar_args(c);
+    a.transport = 1;
+    a.upwind = convection == ANB_CONVECTION_UPWIND;
+    a.nonorth = nonorth != 0;
+    a.flux = flux ? c->sFlux : nullptr;
+    a.sp = c->sSp;
+    a.val = c->mval;
+    a.diag = c->mdiag;
+    a.rhs = c->rhs;
+    const int nOuter = nonorth ? std::max(nNonOrthCorr, 0) + 1 : 1;
+    BicgArgs b{};
+    b.A = mom_sell(c);
+    b.nc = 1;
+    b.b = c->rhs;
+    b.x = c->sPhi;
+    b.r = c->bw[0]; b.rh = c->bw[1]; b.p = c->bw[2]; b.v = c->bw[3];
+    b.s = c->bw[4]; b.t = c->bw[5]; b.ph = c->bw[6]; b.sh = c->bw[7];
+    b.sc = c->scal + kScalBicg;
+    b.fl = c->flags + kFlagBicg;
+    b.atol = absTol;
+    b.rtol = relTol;
+    b.maxit = maxIter;
+    b.red = c->red;
+    int its = 0;
+    bool allConv = true;
+    for (int outer = 0; outer < nOuter; ++outer) {
+      if (a.nonorth) launch_scalar_grad(c->lc, c->dm, a);
+      launch_scalar_assemble(c->lc, c->dm, a);
+      bicg_init(c->lc, b);
+      int done = 0;
+      while (true) {
+        for (int k = 0; k < 16; ++k) bicg_iteration(c->lc, b);
+        done += 16;
+        poll(c, b.fl, 4);
+        if (c->hFlags[0] || done > maxIter + 2) break;
+      }
+      its = c->hFlags[2];
+      allConv = allConv && c->hFlags[3] != 0;
+    }
+    double sc[8];
+    CK(cudaMemcpyAsync(sc, c->scal + kScalBicg, sizeof(sc), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    download_cells1(c, c->sPhi, phi);
+    if (info) {
+      info->iterations = its;
+      info->converged = allConv ? 1 : 0;
+      info->outer = nOuter;
+      info->final_res_norm = sc[5];
+      std::vector<double> hb(c->C);
+      CK(cudaMemcpy(hb.data(), c->rhs, sizeof(double) * c->C, cudaMemcpyDeviceToHost));
+      double bn = 0.0;
+      for (double x : hb) bn += x * x;
+      info->final_rel_res = bn > 0.0 ? sc[5] / std::sqrt(bn) : 0.0;
+    }
+    return allConv ? ANB_OK : ANB_NOT_CONVERGED;
   });
 }
 

@@ -126,6 +126,40 @@ struct PresArgs {
 };
 void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgs& a);
 
+// Scalar elliptic (libpoisson) and steady scalar transport (libscalar) systems on the SIMPLE
+// layout.  Face arrays: internal faces in layout order and orientation, then boundary faces.
+enum ScalarBc : uint8_t {
+  kScalarDirichlet = 0,
+  kScalarNeumann = 1,       // prescribed normal gradient (libpoisson Neumann, libscalar NeumannGradient)
+  kScalarZeroGradient = 2,  // libscalar ZeroGradient
+};
+struct ScalarArgs {
+  const double* phi;      // nCells
+  const double* minv;     // 6 per cell, boundary-type dependent LSQ inverse
+  const uint8_t* bcType;  // nBoundary (ScalarBc)
+  const double* bcVal;    // nBoundary: Dirichlet value or normal gradient
+  const double* bA;       // nBoundary face areas
+  const double* bN;       // 3 per boundary face, unit outward normal
+  const double* gammaF;   // nInternal + nBoundary
+  const double* flux;     // nInternal + nBoundary face flux, or null (no convection)
+  const double* src;      // nCells explicit source per unit volume (f or Su)
+  const double* sp;       // nCells implicit source per unit volume, or null
+  const double* grad;     // 3*nCells SoA gradient of phi
+  int transport;          // 0: libpoisson elliptic rules, 1: libscalar transport rules
+  int upwind;             // transport convection: 0 central, 1 upwind
+  int nonorth;            // add the explicit non-orthogonal correction
+  int refCell;            // layout cell fixed to refValue, -1 for none
+  double refValue;
+  double omega;           // weighted-Jacobi factor for the level-0 smoother weight
+  double* g;              // gradient output (3*nCells)
+  double* val;            // SELL off-diagonals
+  double* diag;
+  double* rhs;
+  double* wdinv;          // omega / diag, or null
+};
+void launch_scalar_grad(const LaunchCfg& lc, const DMesh& m, const ScalarArgs& a);
+void launch_scalar_assemble(const LaunchCfg& lc, const DMesh& m, const ScalarArgs& a);
+
 struct NonOrthArgs {
   const double* rau;
   const double* Gc;   // grad p' (3*nCells SoA)
@@ -157,50 +191,52 @@ void launch_patch_force(cudaStream_t s, const DMesh& m, int b0, int b1, int sign
                         const double* bA, const double* bN, const double* U, const double* P, double* out);
 
 // ---- Krylov ----------------------------------------------------------------------------
-struct BicgArgs {
-  DSell A;
+// T is the storage type of the matrix values and the solver vectors (double: plain method,
+// float: mixed-precision inner solves); scalars, dot products and row sums are double.
+template <class T>
+struct BicgArgsT {
+  DSellT<T> A;
   int nc;             // components (1..3), vectors are nc*n
-  const double* b;
-  double* x;
-  double *r, *rh, *p, *v, *s, *t, *ph, *sh;
+  const T* b;
+  T* x;
+  T *r, *rh, *p, *v, *s, *t, *ph, *sh;
   double* sc;         // per component 8 scalars: rho, rhoN, alpha, omega, eps, rn, tsum, ssum
   int* fl;            // per component 4 ints: done, half, iters, converged
   double atol, rtol;
   int maxit;
   Reducer red;
 };
-void bicg_init(const LaunchCfg& lc, const BicgArgs& a);
-void bicg_iteration(const LaunchCfg& lc, const BicgArgs& a);
+using BicgArgs = BicgArgsT<double>;
+template <class T>
+void bicg_init(const LaunchCfg& lc, const BicgArgsT<T>& a);
+template <class T>
+void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a);
 
-struct AmgDev;  // hierarchy on the device (amg.cu)
-
-struct PcgArgs {
-  DSell A;
-  const double* b;
-  double* x;
-  double *r, *z, *p0, *p1, *q;
+template <class T>
+struct PcgArgsT {
+  DSellT<T> A;
+  const T* b;
+  T* x;
+  T *r, *z, *p0, *p1, *q;
   double* sc;         // rz, alpha, beta, eps, rr, pq
   int* fl;            // done, iters, converged, first
   double atol, rtol;
   int maxit;
   Reducer red;
 };
-void pcg_init(const LaunchCfg& lc, const PcgArgs& a);
-// one iteration; `it` selects the p double buffer; precond == nullptr -> Jacobi
-void pcg_iteration(const LaunchCfg& lc, const PcgArgs& a, int it, const AmgDev* amg);
-// z = M^-1 r for the first iteration (and rz)
-void pcg_precondition(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg);
+using PcgArgs = PcgArgsT<double>;
 
 // ---- AMG (aggregation, V-cycle) ------------------------------------------------------------
-struct AmgLevelDev {
+template <class T>
+struct AmgLevelDevT {
   int n, nc;
   // matrix of this level: level 0 borrows the pressure matrix (SELL-32 slices in sliceOff),
   // coarser levels are CSR (rowOff)
   const int* sliceOff;
   const int* rowOff;
   const int* col;
-  double* val;
-  double* diag;
+  T* val;
+  T* diag;
   // restriction to the next level
   const int* agg;
   const int* memOff;
@@ -209,13 +245,14 @@ struct AmgLevelDev {
   const int* gIdx;
   int nEntNext;        // next level's SELL storage entries
   // work vectors
-  double *b, *x, *x2;
-  double* wdinv;       // omega / diag (Jacobi smoother)
+  T *b, *x, *x2;
+  T* wdinv;            // omega / diag (Jacobi smoother)
 };
-struct AmgDev {
+template <class T>
+struct AmgDevT {
   int nLevels = 0;
-  AmgLevelDev lv[24];
-  double* dense = nullptr;   // coarsest inverse, n_L^2
+  AmgLevelDevT<T> lv[24];
+  double* dense = nullptr;   // coarsest inverse, n_L^2, always double
   int nDense = 0;
   // Jacobi weight and coarse-correction scaling of the symmetric V(1,1)-cycle.  Piecewise-constant
   // prolongation under-estimates smooth error, and scaling the coarse correction (over-correction)
@@ -226,7 +263,39 @@ struct AmgDev {
   cudaGraphExec_t graph = nullptr;  // captured V-cycle (see amg_capture_graph)
   int graphKernels = 0;
 };
-void amg_refresh(const LaunchCfg& lc, AmgDev& amg);  // Galerkin values + dense inverse
-cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgs& a, AmgDev& amg);
+using AmgLevelDev = AmgLevelDevT<double>;
+using AmgDev = AmgDevT<double>;
+
+template <class T>
+void pcg_init(const LaunchCfg& lc, const PcgArgsT<T>& a);
+// one iteration; `it` selects the p double buffer; amg == nullptr -> Jacobi
+template <class T>
+void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgDevT<T>* amg);
+// z = M^-1 r for the first iteration (and rz)
+template <class T>
+void pcg_precondition(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg);
+template <class T>
+void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg);  // Galerkin values + dense inverse
+template <class T>
+cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg);
+
+// ---- mixed-precision defect correction (FP64 outer residual around FP32 inner solves) ------
+// r = b - A x in double with the float matrix, r32 = r, per-component |r|^2 and |b|^2 in
+// sc[8c+0..1]; done flags fl[4c] = |r| <= max(atol, rtol |b|) (nc components of n rows).
+struct DefectArgs {
+  DSellT<float> A;
+  int nc;
+  const double* b;
+  const double* x;
+  float* r32;
+  double* sc;
+  int* fl;
+  const int* frozen;  // nc flags: components not solved (residual not needed), or null
+  double atol, rtol;
+  Reducer red;
+};
+void launch_defect(const LaunchCfg& lc, const DefectArgs& a);
+// x += dx (nc*n), dx = 0
+void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, float* dx);
 
 }  // namespace anb

@@ -11,25 +11,6 @@ namespace anb {
 
 namespace {
 
-__device__ __forceinline__ int row_base(const DMesh& m, int r, int& width) {
-  const int s = r >> 5;
-  const int b = __ldg(&m.sliceOff[s]);
-  width = (__ldg(&m.sliceOff[s + 1]) - b) >> 5;
-  return b + (r & 31);
-}
-
-__device__ __forceinline__ void load_face(const FaceRec* F, int f, double& lam, double& g, double t[3], double d[3]) {
-  const double2* p = reinterpret_cast<const double2*>(F + f);
-  const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), e = __ldg(p + 3);
-  lam = a.x; g = a.y; t[0] = b.x; t[1] = b.y; t[2] = c.x; d[0] = c.y; d[1] = e.x; d[2] = e.y;
-}
-
-__device__ __forceinline__ void load_bnd(const BndRec* B, int b, double& g, double t[3], double S[3], double d[3]) {
-  const double2* p = reinterpret_cast<const double2*>(B + b);
-  const double2 a = __ldg(p), c = __ldg(p + 1), e = __ldg(p + 2), h = __ldg(p + 3), k = __ldg(p + 4);
-  g = a.x; t[0] = a.y; t[1] = c.x; t[2] = c.y; S[0] = e.x; S[1] = e.y; S[2] = h.x; d[0] = h.y; d[1] = k.x; d[2] = k.y;
-}
-
 // ---- least-squares gradient: main.cu:1403-1440 on the moments of main.cu:1159-1251 ----------
 template <int NF>
 __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {

@@ -6,6 +6,11 @@
 // (deterministic block-order combination), which also advances the recurrence scalars and the
 // convergence flags.  Kernels return immediately once their system is converged, so the host
 // can enqueue several iterations between polls without changing the arithmetic.
+//
+// Every kernel is a template over T, the storage type of matrix values and solver vectors:
+// double for the plain method, float for the inner solves of the mixed-precision method (inside
+// an FP64 defect correction, bottom of this file).  Row sums, dot products and recurrence
+// scalars are double in both.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -15,35 +20,42 @@
 namespace anb {
 namespace {
 
+template <class T>
+__device__ __forceinline__ double ld(const T* p) {
+  return (double)__ldg(p);
+}
+
 // y = (D + Off) x for one row of a SELL-32 matrix
-__device__ __forceinline__ double sell_row(const DSell& A, int r, const double* x) {
+template <class T, class X>
+__device__ __forceinline__ double sell_row(const DSellT<T>& A, int r, const X* x) {
   const int s = r >> 5;
   const int b = __ldg(&A.sliceOff[s]) + (r & 31);
   const int W = (__ldg(&A.sliceOff[s + 1]) - __ldg(&A.sliceOff[s])) >> 5;
-  double y = A.diag[r] * x[r];
+  double y = (double)A.diag[r] * (double)x[r];
 #pragma unroll 4
   for (int k = 0; k < W; ++k) {
     const int e = b + (k << 5);
-    y += __ldg(&A.val[e]) * x[__ldg(&A.col[e])];
+    y += ld(&A.val[e]) * (double)x[__ldg(&A.col[e])];
   }
   return y;
 }
 
 // y_c = (D + Off) x_c for up to three vectors sharing one pass over the matrix row
-__device__ __forceinline__ void sell_row3(const DSell& A, int r, const double* x, size_t n, const bool* act, int nc,
+template <class T>
+__device__ __forceinline__ void sell_row3(const DSellT<T>& A, int r, const T* x, size_t n, const bool* act, int nc,
                                           double* y) {
   const int s = r >> 5;
   const int b = __ldg(&A.sliceOff[s]) + (r & 31);
   const int W = (__ldg(&A.sliceOff[s + 1]) - __ldg(&A.sliceOff[s])) >> 5;
-  const double d = A.diag[r];
-  for (int c = 0; c < 3; ++c) y[c] = (c < nc && act[c]) ? d * x[c * n + r] : 0.0;
+  const double d = (double)A.diag[r];
+  for (int c = 0; c < 3; ++c) y[c] = (c < nc && act[c]) ? d * (double)x[c * n + r] : 0.0;
 #pragma unroll 2
   for (int k = 0; k < W; ++k) {
     const int e = b + (k << 5);
-    const double v = __ldg(&A.val[e]);
+    const double v = ld(&A.val[e]);
     const int j = __ldg(&A.col[e]);
     for (int c = 0; c < 3; ++c)
-      if (c < nc && act[c]) y[c] += v * x[c * n + j];
+      if (c < nc && act[c]) y[c] += v * (double)x[c * n + j];
   }
 }
 
@@ -57,20 +69,22 @@ __device__ __forceinline__ bool all_done(const int* fl, int nc) {
   return true;
 }
 
-__global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgsT<T> a) {
   __shared__ double sm[6 * 32];
   const int n = a.A.n;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     for (int c = 0; c < a.nc; ++c) {
       const size_t o = (size_t)c * n;
-      const double rr = a.b[o + r] - sell_row(a.A, r, a.x + o);
-      a.r[o + r] = rr;
-      a.rh[o + r] = rr;
-      a.p[o + r] = 0.0;
-      a.v[o + r] = 0.0;
+      const double bb = (double)a.b[o + r];
+      const double rr = bb - sell_row(a.A, r, a.x + o);
+      a.r[o + r] = (T)rr;
+      a.rh[o + r] = (T)rr;
+      a.p[o + r] = T(0);
+      a.v[o + r] = T(0);
       acc[2 * c] += rr * rr;
-      acc[2 * c + 1] += a.b[o + r] * a.b[o + r];
+      acc[2 * c + 1] += bb * bb;
     }
   }
   if (grid_reduce<6>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
@@ -93,7 +107,8 @@ __global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgs a) {
 }
 
 // p = r + beta (p - omega v); ph = D^-1 p
-__global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgsT<T> a) {
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
   double beta[3], om[3];
@@ -105,19 +120,20 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgs a) {
     om[c] = s[3];
   }
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const double dinv = 1.0 / a.A.diag[r];
+    const double dinv = 1.0 / (double)a.A.diag[r];
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
-      const double pn = a.r[i] + beta[c] * (a.p[i] - om[c] * a.v[i]);
-      a.p[i] = pn;
-      a.ph[i] = dinv * pn;
+      const double pn = (double)a.r[i] + beta[c] * ((double)a.p[i] - om[c] * (double)a.v[i]);
+      a.p[i] = (T)pn;
+      a.ph[i] = (T)(dinv * pn);
     }
   }
 }
 
 // v = A ph ; alpha = rhoN / (rh . v) ; rho = rhoN
-__global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgsT<T> a) {
   __shared__ double sm[3 * 32];
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
@@ -130,8 +146,8 @@ __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgs a) {
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
-      a.v[o + r] = y[c];
-      acc[c] += a.rh[o + r] * y[c];
+      a.v[o + r] = (T)y[c];
+      acc[c] += (double)a.rh[o + r] * y[c];
     }
   }
   if (grid_reduce<3>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
@@ -149,7 +165,8 @@ __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgs a) {
 }
 
 // s = r - alpha v ; sh = D^-1 s ; early exit if |s| <= eps
-__global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgsT<T> a) {
   __shared__ double sm[3 * 32];
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
@@ -161,13 +178,13 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgs a) {
   }
   double acc[3] = {0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const double dinv = 1.0 / a.A.diag[r];
+    const double dinv = 1.0 / (double)a.A.diag[r];
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
-      const double sv = a.r[i] - al[c] * a.v[i];
-      a.s[i] = sv;
-      a.sh[i] = dinv * sv;
+      const double sv = (double)a.r[i] - al[c] * (double)a.v[i];
+      a.s[i] = (T)sv;
+      a.sh[i] = (T)(dinv * sv);
       acc[c] += sv * sv;
     }
   }
@@ -180,7 +197,8 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgs a) {
 }
 
 // t = A sh ; omega = (t.s)/(t.t)
-__global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgsT<T> a) {
   __shared__ double sm[6 * 32];
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
@@ -194,8 +212,8 @@ __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgs a) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
       const double tv = y[c];
-      a.t[o + r] = tv;
-      acc[2 * c] += tv * a.s[o + r];
+      a.t[o + r] = (T)tv;
+      acc[2 * c] += tv * (double)a.s[o + r];
       acc[2 * c + 1] += tv * tv;
     }
   }
@@ -208,7 +226,8 @@ __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgs a) {
 }
 
 // x += alpha ph + omega sh ; r = s - omega t ; convergence
-__global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgsT<T> a) {
   __shared__ double sm[6 * 32];
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
@@ -226,13 +245,13 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgs a) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
       if (half[c]) {
-        a.x[i] += al[c] * a.ph[i];
+        a.x[i] = (T)((double)a.x[i] + al[c] * (double)a.ph[i]);
       } else {
-        a.x[i] += al[c] * a.ph[i] + om[c] * a.sh[i];
-        const double rr = a.s[i] - om[c] * a.t[i];
-        a.r[i] = rr;
+        a.x[i] = (T)((double)a.x[i] + al[c] * (double)a.ph[i] + om[c] * (double)a.sh[i]);
+        const double rr = (double)a.s[i] - om[c] * (double)a.t[i];
+        a.r[i] = (T)rr;
         acc[2 * c] += rr * rr;
-        acc[2 * c + 1] += a.rh[i] * rr;
+        acc[2 * c + 1] += (double)a.rh[i] * rr;
       }
     }
   }
@@ -263,15 +282,17 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgs a) {
 // ---------------------------------------------------------------- PCG
 // sc: 0 rz, 1 alpha, 2 beta, 3 eps, 4 rr, 5 pq ; fl: 0 done, 1 iters, 2 converged, 3 first
 
-__global__ void __launch_bounds__(kBlock) k_pcg_init(PcgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_pcg_init(PcgArgsT<T> a) {
   __shared__ double sm[2 * 32];
   const int n = a.A.n;
   double acc[2] = {0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const double rr = a.b[r] - sell_row(a.A, r, a.x);
-    a.r[r] = rr;
+    const double bb = (double)a.b[r];
+    const double rr = bb - sell_row(a.A, r, a.x);
+    a.r[r] = (T)rr;
     acc[0] += rr * rr;
-    acc[1] += a.b[r] * a.b[r];
+    acc[1] += bb * bb;
   }
   if (grid_reduce<2>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
     a.sc[3] = fmax(a.atol, a.rtol * sqrt(acc[1]));
@@ -285,15 +306,16 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(PcgArgs a) {
 }
 
 // Jacobi preconditioner z = D^-1 r with rz (used when the AMG is off)
-__global__ void __launch_bounds__(kBlock) k_pcg_jacobi(PcgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_pcg_jacobi(PcgArgsT<T> a) {
   __shared__ double sm[32];
   if (a.fl[0]) return;
   const int n = a.A.n;
   double acc[1] = {0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const double z = a.r[r] / a.A.diag[r];
-    a.z[r] = z;
-    acc[0] += a.r[r] * z;
+    const double z = (double)a.r[r] / (double)a.A.diag[r];
+    a.z[r] = (T)z;
+    acc[0] += (double)a.r[r] * z;
   }
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
     const double rzOld = a.sc[0];
@@ -303,7 +325,8 @@ __global__ void __launch_bounds__(kBlock) k_pcg_jacobi(PcgArgs a) {
 }
 
 // pNew = z + beta pOld (rows and, on the fly, their neighbours); q = A pNew; alpha = rz / (p.q)
-__global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgs a, const double* pOld, double* pNew) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld, T* pNew) {
   __shared__ double sm[32];
   if (a.fl[0]) return;
   const int n = a.A.n;
@@ -313,15 +336,15 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgs a, const double* pOld
     const int s = r >> 5;
     const int b = __ldg(&a.A.sliceOff[s]) + (r & 31);
     const int W = (__ldg(&a.A.sliceOff[s + 1]) - __ldg(&a.A.sliceOff[s])) >> 5;
-    const double pr = a.z[r] + beta * pOld[r];
-    double q = a.A.diag[r] * pr;
+    const double pr = (double)(T)((double)a.z[r] + beta * (double)pOld[r]);
+    double q = (double)a.A.diag[r] * pr;
     for (int k = 0; k < W; ++k) {
       const int e = b + (k << 5);
       const int c = __ldg(&a.A.col[e]);
-      q += a.A.val[e] * (a.z[c] + beta * pOld[c]);
+      q += (double)a.A.val[e] * (double)(T)((double)a.z[c] + beta * (double)pOld[c]);
     }
-    pNew[r] = pr;
-    a.q[r] = q;
+    pNew[r] = (T)pr;
+    a.q[r] = (T)q;
     acc[0] += pr * q;
   }
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
@@ -332,16 +355,17 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgs a, const double* pOld
 }
 
 // x += alpha p ; r -= alpha q ; convergence test on |r|
-__global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgs a, const double* p) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgsT<T> a, const T* p) {
   __shared__ double sm[32];
   if (a.fl[0]) return;
   const int n = a.A.n;
   const double al = a.sc[1];
   double acc[1] = {0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    a.x[r] += al * p[r];
-    const double rr = a.r[r] - al * a.q[r];
-    a.r[r] = rr;
+    a.x[r] = (T)((double)a.x[r] + al * (double)p[r]);
+    const double rr = (double)a.r[r] - al * (double)a.q[r];
+    a.r[r] = (T)rr;
     acc[0] += rr * rr;
   }
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
@@ -361,12 +385,13 @@ __global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgs a, const double* p) {
 // Down, part 1: weighted-Jacobi pre-smoothing from zero (x = w D^-1 b) fused with the residual
 // r = b - A x (neighbour x computed on the fly); thread per row, SELL-coalesced.  r goes to x2,
 // which is free until the up sweep.
-__global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelDev f, double omega) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelDevT<T> f, double omega) {
   if (*done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
-    const double di = __ldg(&f.diag[i]);
-    const double bi = __ldg(&f.b[i]);
-    const double xi = __ldg(&f.wdinv[i]) * bi;
+    const double di = ld(&f.diag[i]);
+    const double bi = ld(&f.b[i]);
+    const double xi = ld(&f.wdinv[i]) * bi;
     double ax = di * xi;
     const int s = i >> 5;
     const int b = __ldg(&f.sliceOff[s]) + (i & 31);
@@ -375,10 +400,10 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
     for (int k = 0; k < W; ++k) {
       const int e = b + (k << 5);
       const int j = __ldg(&f.col[e]);
-      ax += __ldg(&f.val[e]) * (__ldg(&f.wdinv[j]) * __ldg(&f.b[j]));
+      ax += ld(&f.val[e]) * (ld(&f.wdinv[j]) * ld(&f.b[j]));
     }
-    f.x[i] = xi;
-    f.x2[i] = bi - ax;
+    f.x[i] = (T)xi;
+    f.x2[i] = (T)(bi - ax);
   }
 }
 
@@ -393,8 +418,8 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-template <int G>
-__global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLevelDev f, double omega) {
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLevelDevT<T> f, double omega) {
   if (*done) return;
   const int lane = threadIdx.x & 31, sub = lane % G;
   const int rowsPerWarp = 32 / G;
@@ -407,22 +432,22 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLe
       const int k1 = __ldg(&f.rowOff[i + 1]);
       for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
         const int j = __ldg(&f.col[k]);
-        acc += __ldg(&f.val[k]) * (__ldg(&f.wdinv[j]) * __ldg(&f.b[j]));
+        acc += ld(&f.val[k]) * (ld(&f.wdinv[j]) * ld(&f.b[j]));
       }
     }
     acc = group_sum<G>(acc);
     if (i < f.n && sub == 0) {
-      const double di = __ldg(&f.diag[i]), bi = __ldg(&f.b[i]);
-      const double xi = __ldg(&f.wdinv[i]) * bi;
-      f.x[i] = xi;
-      f.x2[i] = bi - di * xi - acc;
+      const double di = ld(&f.diag[i]), bi = ld(&f.b[i]);
+      const double xi = ld(&f.wdinv[i]) * bi;
+      f.x[i] = (T)xi;
+      f.x2[i] = (T)(bi - di * xi - acc);
     }
   }
 }
 
-template <int G>
-__global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevelDev f, const double* e, double omega,
-                                                       double corr, double* out) {
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevelDevT<T> f, const T* e, double omega,
+                                                       double corr, T* out) {
   if (*done) return;
   const int lane = threadIdx.x & 31, sub = lane % G;
   const int rowsPerWarp = 32 / G;
@@ -435,41 +460,43 @@ __global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevel
       const int k1 = __ldg(&f.rowOff[i + 1]);
       for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
         const int j = __ldg(&f.col[k]);
-        acc += __ldg(&f.val[k]) * (__ldg(&f.x[j]) + corr * __ldg(&e[__ldg(&f.agg[j])]));
+        acc += ld(&f.val[k]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
       }
     }
     acc = group_sum<G>(acc);
     if (i < f.n && sub == 0) {
-      const double di = __ldg(&f.diag[i]);
-      const double xi = __ldg(&f.x[i]) + corr * __ldg(&e[__ldg(&f.agg[i])]);
-      out[i] = xi + __ldg(&f.wdinv[i]) * (__ldg(&f.b[i]) - di * xi - acc);
+      const double di = ld(&f.diag[i]);
+      const double xi = ld(&f.x[i]) + corr * ld(&e[__ldg(&f.agg[i])]);
+      out[i] = (T)(xi + ld(&f.wdinv[i]) * (ld(&f.b[i]) - di * xi - acc));
     }
   }
 }
 
 // Down, part 2: piecewise-constant restriction b_next[I] = sum of r over the rows of I.
-__global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLevelDev f, double* bNext) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLevelDevT<T> f, T* bNext) {
   if (*done) return;
   for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < f.nc; I += gridDim.x * blockDim.x) {
     double acc = 0.0;
     const int m1 = __ldg(&f.memOff[I + 1]);
 #pragma unroll 4
-    for (int mm = __ldg(&f.memOff[I]); mm < m1; ++mm) acc += f.x2[__ldg(&f.mem[mm])];
-    bNext[I] = acc;
+    for (int mm = __ldg(&f.memOff[I]); mm < m1; ++mm) acc += (double)f.x2[__ldg(&f.mem[mm])];
+    bNext[I] = (T)acc;
   }
 }
 
 // Up: prolongate the coarse correction and post-smooth (one weighted-Jacobi sweep) in one pass:
 // xt_j = x_j + corr * e[agg(j)] on the fly, out_i = xt_i + w D^-1 (b_i - (A xt)_i).
 // On level 0 it also forms r.z for the PCG recurrence.
-__global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevelDev f, const double* e, double omega,
-                                                   double corr, double* out, int finest, PcgArgs a) {
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevelDevT<T> f, const T* e, double omega,
+                                                   double corr, T* out, int finest, PcgArgsT<T> a) {
   __shared__ double sm[32];
   if (*doneFlag) return;
   double acc[1] = {0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
-    const double di = __ldg(&f.diag[i]);
-    const double xi = __ldg(&f.x[i]) + corr * __ldg(&e[__ldg(&f.agg[i])]);
+    const double di = ld(&f.diag[i]);
+    const double xi = ld(&f.x[i]) + corr * ld(&e[__ldg(&f.agg[i])]);
     double ax = di * xi;
     const int s = i >> 5;
     const int b = __ldg(&f.sliceOff[s]) + (i & 31);
@@ -479,11 +506,12 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
     for (int k = 0; k < W; ++k) {
       const int ee = b + (k << 5);
       const int j = __ldg(&f.col[ee]);
-      ax += __ldg(&f.val[ee]) * (__ldg(&f.x[j]) + corr * __ldg(&e[__ldg(&f.agg[j])]));
+      ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
     }
-    const double xn = xi + __ldg(&f.wdinv[i]) * (__ldg(&f.b[i]) - ax);
+    const double bi = (double)f.b[i];
+    const T xn = (T)(xi + ld(&f.wdinv[i]) * (bi - ax));
     out[i] = xn;
-    if (finest) acc[0] += f.b[i] * xn;
+    if (finest) acc[0] += bi * (double)xn;
   }
   if (!finest) return;
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
@@ -493,52 +521,53 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
   }
 }
 
-// Coarsest level: x = A^-1 b with the stored dense inverse (one block).  The inverse of the SPD
-// coarse matrix is symmetric, so thread i walks column i: consecutive threads read consecutive
-// addresses.
-__global__ void k_amg_dense_apply(const int* done, int n, const double* inv, const double* b, double* x) {
+// Coarsest level: x = A^-1 b with the stored dense inverse (double, one block), warp per row.
+template <class T>
+__global__ void k_amg_dense_apply(const int* done, int n, const double* inv, const T* b, T* x) {
   if (*done) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int i = w; i < n; i += nw) {  // warp per row, lanes across the row (coalesced)
+  for (int i = w; i < n; i += nw) {  // lanes across the row (coalesced)
     double s = 0.0;
-    for (int j = lane; j < n; j += 32) s += __ldg(&inv[(size_t)i * n + j]) * __ldg(&b[j]);
+    for (int j = lane; j < n; j += 32) s += __ldg(&inv[(size_t)i * n + j]) * ld(&b[j]);
     s = warp_sum(s);
-    if (lane == 0) x[i] = s;
+    if (lane == 0) x[i] = (T)s;
   }
 }
 
-// Galerkin values of the next level: one gather list per coarse storage entry.
-__global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDev f, double* valNext, double* diagNext,
-                                                         double* wdinvNext, double omega) {
+// Galerkin values of the next level: one gather list per coarse storage entry (sums in double).
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDevT<T> f, T* valNext, T* diagNext, T* wdinvNext,
+                                                         double omega) {
   const int nT = f.nEntNext + f.nc;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nT; t += gridDim.x * blockDim.x) {
     double s = 0.0;
     for (int k = f.gOff[t]; k < f.gOff[t + 1]; ++k) {
       const int idx = f.gIdx[k];
-      s += idx >= 0 ? f.val[idx] : f.diag[-1 - idx];
+      s += idx >= 0 ? (double)f.val[idx] : (double)f.diag[-1 - idx];
     }
     if (t < f.nEntNext) {
-      valNext[t] = s;
+      valNext[t] = (T)s;
     } else {
-      diagNext[t - f.nEntNext] = s;
-      wdinvNext[t - f.nEntNext] = omega / s;
+      diagNext[t - f.nEntNext] = (T)s;
+      wdinvNext[t - f.nEntNext] = (T)(omega / s);
     }
   }
 }
 
-// Dense inverse of the coarsest matrix by in-place Gauss-Jordan (SPD, no pivoting needed);
-// a pivot below 1e-13 of the largest diagonal (singular, all-Neumann systems) gets a zero
-// row/column, i.e. the correction ignores the null direction.  One block, shared memory.
-__global__ void k_amg_dense_factor(AmgLevelDev c, double* inv) {
+// Dense inverse of the coarsest matrix by in-place Gauss-Jordan in double (SPD, no pivoting
+// needed); a pivot below 1e-13 of the largest diagonal (singular, all-Neumann systems) gets a
+// zero row/column, i.e. the correction ignores the null direction.  One block, shared memory.
+template <class T>
+__global__ void k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
   extern __shared__ double A[];
   const int n = c.n;
   for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = 0.0;
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) {  // the coarsest level is always CSR
-    A[i * n + i] = c.diag[i];
+    A[i * n + i] = (double)c.diag[i];
     for (int k = c.rowOff[i]; k < c.rowOff[i + 1]; ++k) {
       const int j = c.col[k];
-      if (j != i) A[i * n + j] += c.val[k];
+      if (j != i) A[i * n + j] += (double)c.val[k];
     }
   }
   __syncthreads();
@@ -583,83 +612,129 @@ __global__ void k_amg_dense_factor(AmgLevelDev c, double* inv) {
   for (int t = threadIdx.x; t < n * n; t += blockDim.x) inv[t] = A[t];
 }
 
+// ---------------------------------------------------------------- mixed-precision defect
+// r = b - A x in double (float matrix, double x), r32 = r; per component |r|^2, |b|^2.
+__global__ void __launch_bounds__(kBlock) k_defect(DefectArgs a) {
+  __shared__ double sm[6 * 32];
+  const int n = a.A.n;
+  bool act[3];
+  for (int c = 0; c < 3; ++c) act[c] = c < a.nc && !(a.frozen && a.frozen[c]);
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    for (int c = 0; c < a.nc; ++c) {
+      if (!act[c]) continue;
+      const size_t o = (size_t)c * n;
+      const double bb = a.b[o + r];
+      const double rr = bb - sell_row(a.A, r, a.x + o);
+      a.r32[o + r] = (float)rr;
+      acc[2 * c] += rr * rr;
+      acc[2 * c + 1] += bb * bb;
+    }
+  }
+  if (grid_reduce<6>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
+    for (int c = 0; c < a.nc; ++c) {
+      if (!act[c]) {
+        a.fl[4 * c] = 1;
+        continue;
+      }
+      a.sc[8 * c] = acc[2 * c];
+      a.sc[8 * c + 1] = acc[2 * c + 1];
+      a.fl[4 * c] = sqrt(acc[2 * c]) <= fmax(a.atol, a.rtol * sqrt(acc[2 * c + 1])) ? 1 : 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_apply_correction(size_t n, double* x, float* dx) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] += (double)dx[i];
+    dx[i] = 0.0f;
+  }
+}
+
 }  // namespace
 
-void bicg_init(const LaunchCfg& lc, const BicgArgs& a) {
+template <class T>
+void bicg_init(const LaunchCfg& lc, const BicgArgsT<T>& a) {
   g_launches += 1;
-  k_bicg_init<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  k_bicg_init<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
-void bicg_iteration(const LaunchCfg& lc, const BicgArgs& a) {
+template <class T>
+void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
+  const double vbytes = lc.ab ? lc.ab->bicg_spmv(a.nc) * (sizeof(T) == 4 ? 0.5 : 1.0) : 0.0;
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
-    k_bicg_p<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    k_bicg_p<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
   {
-    ProfScope ps(lc, kKfBicgSpmv, lc.ab ? lc.ab->bicg_spmv(a.nc) : 0.0);
-    k_bicg_v<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-  }
-  {
-    ProfScope ps(lc, kKfBicgVector, 0.0);
-    k_bicg_s<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-  }
-  {
-    ProfScope ps(lc, kKfBicgSpmv, lc.ab ? lc.ab->bicg_spmv(a.nc) : 0.0);
-    k_bicg_t<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    ProfScope ps(lc, kKfBicgSpmv, vbytes);
+    k_bicg_v<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
-    k_bicg_x<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    k_bicg_s<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
+  {
+    ProfScope ps(lc, kKfBicgSpmv, vbytes);
+    k_bicg_t<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  }
+  {
+    ProfScope ps(lc, kKfBicgVector, 0.0);
+    k_bicg_x<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
 }
 
-void pcg_init(const LaunchCfg& lc, const PcgArgs& a) {
+template <class T>
+void pcg_init(const LaunchCfg& lc, const PcgArgsT<T>& a) {
   g_launches += 1;
-  k_pcg_init<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  k_pcg_init<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
 
 static int blocks_for(int n, int cap) { return std::max(1, std::min(cap, (n + kBlock - 1) / kBlock)); }
 
 constexpr int kCoarseLanes = 8;  // lanes per row on the CSR coarse levels
 
-static void vcycle(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
+template <class T>
+static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
   const int L = amg->nLevels;
   // level 0 right-hand side is the PCG residual
   {
-    const AmgLevelDev& f = amg->lv[0];
+    const AmgLevelDevT<T>& f = amg->lv[0];
     ProfScope ps(lc, kKfAmgResid0, 0.0, 2);
-    k_amg_resid<<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
-    k_amg_restrict<<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
+    k_amg_resid<T><<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+    k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
     ProfScope ps(lc, kKfAmgCoarse, 0.0, 3 * L - 6);
     for (int l = 1; l + 1 < L; ++l) {
-      const AmgLevelDev& f = amg->lv[l];
-      k_amg_resid_csr<kCoarseLanes><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
+      const AmgLevelDevT<T>& f = amg->lv[l];
+      k_amg_resid_csr<kCoarseLanes, T><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, amg->omega);
-      k_amg_restrict<<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
+      k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
     }
-    const AmgLevelDev& c = amg->lv[L - 1];
-    k_amg_dense_apply<<<1, 1024, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
+    const AmgLevelDevT<T>& c = amg->lv[L - 1];
+    k_amg_dense_apply<T><<<1, 1024, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
     for (int l = L - 2; l >= 1; --l) {
-      const AmgLevelDev& f = amg->lv[l];
+      const AmgLevelDevT<T>& f = amg->lv[l];
       // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
-      const double* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
-      k_amg_up_csr<kCoarseLanes><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
+      const T* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
+      k_amg_up_csr<kCoarseLanes, T><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, e, amg->omega, amg->corr, f.x2);
     }
   }
   {
-    const AmgLevelDev& f = amg->lv[0];
-    const double* e = (L == 2) ? amg->lv[1].x : amg->lv[1].x2;
+    const AmgLevelDevT<T>& f = amg->lv[0];
+    const T* e = (L == 2) ? amg->lv[1].x : amg->lv[1].x2;
     ProfScope ps(lc, kKfAmgUp0, 0.0);
-    k_amg_up<<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
+    k_amg_up<T><<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1,
+                                                                          a);
   }
 }
 
-void pcg_precondition(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) {
+template <class T>
+void pcg_precondition(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
   if (!amg || amg->nLevels < 2) {
     g_launches += 1;
-    k_pcg_jacobi<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    k_pcg_jacobi<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   } else if (amg->graph) {
     g_launches += amg->graphKernels;
     cudaGraphLaunch(amg->graph, lc.stream);
@@ -671,7 +746,8 @@ void pcg_precondition(const LaunchCfg& lc, const PcgArgs& a, const AmgDev* amg) 
 // Records one V-cycle into a CUDA graph.  Every pointer and scalar the V-cycle kernels read is
 // fixed for the life of the hierarchy (values change on refresh, addresses do not), so the
 // graph is captured once and replayed for every preconditioner application.
-cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgs& a, AmgDev& amg) {
+template <class T>
+cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
   if (amg.graph) {
     cudaGraphExecDestroy(amg.graph);
     amg.graph = nullptr;
@@ -692,33 +768,60 @@ cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgs& a, AmgDev& amg
   return e;
 }
 
-void pcg_iteration(const LaunchCfg& lc, const PcgArgs& a, int it, const AmgDev* amg) {
-  const double* pOld = (it & 1) ? a.p1 : a.p0;
-  double* pNew = (it & 1) ? a.p0 : a.p1;
+template <class T>
+void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgDevT<T>* amg) {
+  const T* pOld = (it & 1) ? a.p1 : a.p0;
+  T* pNew = (it & 1) ? a.p0 : a.p1;
   {
-    ProfScope ps(lc, kKfPcgSpmv, lc.ab ? lc.ab->pcg_spmv() : 0.0);
-    k_pcg_pq<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+    // algorithmic bytes: 12 B per off-diagonal (value + column) and 40 B per row in FP64;
+    // values and vectors halve in FP32
+    const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
+    ProfScope ps(lc, kKfPcgSpmv, by);
+    k_pcg_pq<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
   }
   {
     ProfScope ps(lc, kKfPcgUpdate, 0.0);
-    k_pcg_xr<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pNew);
+    k_pcg_xr<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pNew);
   }
   pcg_precondition(lc, a, amg);
 }
 
-void amg_refresh(const LaunchCfg& lc, AmgDev& amg) {
+template <class T>
+void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg) {
   for (int l = 0; l + 1 < amg.nLevels; ++l) {
-    AmgLevelDev& f = amg.lv[l];
-    AmgLevelDev& c = amg.lv[l + 1];
+    AmgLevelDevT<T>& f = amg.lv[l];
+    AmgLevelDevT<T>& c = amg.lv[l + 1];
     g_launches += 1;
-    k_amg_galerkin<<<blocks_for(f.nEntNext + f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(f, c.val, c.diag,
-                                                                                          c.wdinv, amg.omega);
+    k_amg_galerkin<T><<<blocks_for(f.nEntNext + f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(f, c.val, c.diag,
+                                                                                             c.wdinv, amg.omega);
   }
-  const AmgLevelDev& c = amg.lv[amg.nLevels - 1];
+  const AmgLevelDevT<T>& c = amg.lv[amg.nLevels - 1];
   const size_t smem = sizeof(double) * (size_t)c.n * c.n;
-  cudaFuncSetAttribute(k_amg_dense_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_amg_dense_factor<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   g_launches += 1;
-  k_amg_dense_factor<<<1, 1024, smem, lc.stream>>>(c, amg.dense);
+  k_amg_dense_factor<T><<<1, 1024, smem, lc.stream>>>(c, amg.dense);
 }
+
+void launch_defect(const LaunchCfg& lc, const DefectArgs& a) {
+  g_launches += 1;
+  k_defect<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+}
+
+void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, float* dx) {
+  g_launches += 1;
+  k_apply_correction<<<lc.rowBlocks, kBlock, 0, lc.stream>>>((size_t)n * nc, x, dx);
+}
+
+#define ANB_INSTANTIATE(T)                                                                    \
+  template void bicg_init<T>(const LaunchCfg&, const BicgArgsT<T>&);                          \
+  template void bicg_iteration<T>(const LaunchCfg&, const BicgArgsT<T>&);                     \
+  template void pcg_init<T>(const LaunchCfg&, const PcgArgsT<T>&);                            \
+  template void pcg_iteration<T>(const LaunchCfg&, const PcgArgsT<T>&, int, const AmgDevT<T>*); \
+  template void pcg_precondition<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*);  \
+  template void amg_refresh<T>(const LaunchCfg&, AmgDevT<T>&);                                \
+  template cudaError_t amg_capture_graph<T>(const LaunchCfg&, const PcgArgsT<T>&, AmgDevT<T>&);
+ANB_INSTANTIATE(double)
+ANB_INSTANTIATE(float)
+#undef ANB_INSTANTIATE
 
 }  // namespace anb

@@ -295,4 +295,67 @@ Layout build_layout(const HostMesh& m) {
   return L;
 }
 
+std::vector<double> scalar_lsq_minv(const HostMesh& m, const Layout& L, const std::vector<uint8_t>& bDirichlet) {
+  const int C = m.nCells, nI = m.nInternalFaces, nF = m.nFaces;
+  if ((int)bDirichlet.size() != nF - nI) throw std::runtime_error("scalar_lsq_minv: boundary type size mismatch");
+  // sorted unique neighbours (cellNbrs) and ascending boundary faces (cellBFace) per cell
+  std::vector<int> off(C + 1, 0), adj;
+  for (int f = 0; f < nI; ++f) {
+    ++off[m.owner[f] + 1];
+    ++off[m.neigh[f] + 1];
+  }
+  for (int c = 0; c < C; ++c) off[c + 1] += off[c];
+  adj.resize(off[C]);
+  {
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int f = 0; f < nI; ++f) {
+      adj[fill[m.owner[f]]++] = m.neigh[f];
+      adj[fill[m.neigh[f]]++] = m.owner[f];
+    }
+  }
+  std::vector<std::vector<int>> cellB(C);
+  for (int f = nI; f < nF; ++f) cellB[m.owner[f]].push_back(f);
+  std::vector<double> out((size_t)6 * C, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int P = 0; P < C; ++P) {
+    std::sort(adj.begin() + off[P], adj.begin() + off[P + 1]);
+    const Vec3 xP = m.cc[P];
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    auto acc = [&](const double r[3]) {
+      const double w = 1.0 / std::max(r[0] * r[0] + r[1] * r[1] + r[2] * r[2], 1e-30);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) M[i][j] += w * r[i] * r[j];
+    };
+    for (int k = off[P]; k < off[P + 1]; ++k) {
+      const Vec3& x = m.cc[adj[k]];
+      const double r[3] = {x[0] - xP[0], x[1] - xP[1], x[2] - xP[2]};
+      acc(r);
+    }
+    for (int f : cellB[P]) {
+      const double rcf[3] = {m.xf[f][0] - xP[0], m.xf[f][1] - xP[1], m.xf[f][2] - xP[2]};
+      if (bDirichlet[f - nI]) {
+        acc(rcf);
+      } else {
+        const Vec3& n = m.nf[f];
+        const double dn = std::max(rcf[0] * n[0] + rcf[1] * n[1] + rcf[2] * n[2], 1e-30);
+        const double r[3] = {dn * n[0], dn * n[1], dn * n[2]};
+        acc(r);
+      }
+    }
+    const double a = M[0][0], b = M[0][1], c = M[0][2], d = M[1][0], e = M[1][1], f2 = M[1][2], g = M[2][0],
+                 h = M[2][1], k = M[2][2];
+    const double det = a * (e * k - f2 * h) - b * (d * k - f2 * g) + c * (d * h - e * g);
+    double* o = &out[(size_t)6 * L.old2new[P]];
+    if (std::fabs(det) > 1e-20) {
+      o[0] = (e * k - f2 * h) / det;
+      o[1] = (c * h - b * k) / det;
+      o[2] = (b * f2 - c * e) / det;
+      o[3] = (a * k - c * g) / det;
+      o[4] = (c * d - a * f2) / det;
+      o[5] = (a * e - b * d) / det;
+    }
+  }
+  return out;
+}
+
 }  // namespace anb

@@ -64,6 +64,13 @@ struct Layout {
 // Throws std::runtime_error when two internal faces join the same pair of cells (not supported).
 Layout build_layout(const HostMesh& m);
 
+// LSQ moment inverse of the scalar libraries (libpoisson/src/gradient.cu:21-83,
+// libscalar/src/scalar_transport_library.cu:185-246): neighbours as in the SIMPLE operator,
+// Dirichlet boundary faces at the face centre, every other boundary face as the pure-normal
+// constraint r = max((x_f - x_P).n, 1e-30) n.  bDirichlet has one entry per boundary face (input
+// order); the result is 6 per cell in the layout's cell order.
+std::vector<double> scalar_lsq_minv(const HostMesh& m, const Layout& L, const std::vector<uint8_t>& bDirichlet);
+
 // Reverse Cuthill-McKee order of an undirected graph in CSR form (new2old).
 std::vector<int> rcm_order(int n, const std::vector<int>& adjOff, const std::vector<int>& adj);
 

@@ -141,6 +141,50 @@ int anb_patch_force(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* 
  * race and must be serialised by the caller. */
 int anb_patch_force_nalloc(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* out);
 
+/* ---- scalar libraries (method-of-manufactured-solutions path) --------------------------------
+ * Both solves run on the context's mesh and leave its SIMPLE state (U, p, phi) untouched; they
+ * reuse the context's matrix storage, so the next SIMPLE step rebuilds its pressure AMG.
+ * Face arrays have nFaces entries in input face order and orientation (internal faces first);
+ * bc_type/bc_value are read at boundary faces only.  Cell arrays have nCells entries. */
+#define ANB_SCALAR_DIRICHLET 0
+#define ANB_SCALAR_NEUMANN 1        /* prescribed normal gradient (libpoisson Neumann,
+                                       libscalar NeumannGradient) */
+#define ANB_SCALAR_ZERO_GRADIENT 2  /* libscalar ZeroGradient (transport only) */
+#define ANB_CONVECTION_CENTRAL 0
+#define ANB_CONVECTION_UPWIND 1
+
+typedef struct anb_solve_info {
+  int iterations;          /* Krylov iterations of the last linear solve */
+  int converged;           /* 1 if every linear solve met its tolerance */
+  int outer;               /* non-orthogonal outer passes done */
+  double final_res_norm;   /* two-norm of the last solve's residual */
+  double final_rel_res;    /* final_res_norm / two-norm of its right-hand side */
+} anb_solve_info;
+
+/* solve_scalar_elliptic (libpoisson/src/poisson_library.cu:3-47 with the assembly of
+ * scalar_elliptic.cu:60-136 and the gradient of gradient.cu:21-83): -div(gamma grad phi) =
+ * source with gamma per face (NULL: 1, i.e. solve_poisson), nonorth_corr+1 passes of gradient,
+ * assembly and a PCG solve from phi = 0 (one pass when laplacian_nonorth == 0).  The reference
+ * solves with HYPRE PCG + BoomerAMG; this library uses its aggregation-AMG PCG at abs_tol
+ * (two-norm) / rel_tol.  Errors as the reference: a problem with no Dirichlet face needs
+ * use_reference_cell; reference_cell must be a valid cell. */
+int anb_scalar_elliptic_solve(anb_ctx* ctx, const double* gamma_face, const double* cell_source,
+                              const int* bc_type, const double* bc_value, int laplacian_nonorth,
+                              int nonorth_corr, int use_reference_cell, int reference_cell,
+                              double reference_value, double abs_tol, double rel_tol, int max_iter,
+                              double* phi, anb_solve_info* info);
+
+/* solve_steady_scalar_transport (libscalar/src/scalar_transport_library.cu:475-514 with the
+ * assembly of 250-357): div(F phi) - div(gamma grad phi) = Su + Sp phi for a given face flux
+ * (NULL: diffusion only), central or upwind convection, nonorth_corr+1 passes when
+ * diffusion_nonorth != 0, each a Jacobi-preconditioned BiCGSTAB solve starting from the
+ * current phi (x0, or 0 when NULL). */
+int anb_scalar_transport_solve(anb_ctx* ctx, const double* face_flux, const double* gamma_face,
+                               const double* su, const double* sp, const int* bc_type,
+                               const double* bc_value, int convection, int diffusion_nonorth,
+                               int nonorth_corr, double abs_tol, double rel_tol, int max_iter,
+                               const double* x0, double* phi, anb_solve_info* info);
+
 /* ---- measurement (no counterpart in the reference; used by the benchmark) ------------------
  * Kernel families for anb_profile_select: every launch of the selected family is bracketed by
  * CUDA events on the context's stream and its algorithmic (compulsory) bytes are accumulated. */

@@ -59,6 +59,9 @@ def lib() -> ct.CDLL:
         L.orc_simple_run.argtypes = [ct.c_void_p, ct.POINTER(OrcParams), ct.c_int, _dp, _dp, _dp, _dp, _dp,
                                      ct.POINTER(OrcStats)]
         L.orc_patch_force.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_double, _dp, _dp, _dp, _dp, _dp]
+        L.orc_scalar_gradient.argtypes = [ct.c_void_p, _ip, _dp, _dp, _dp, _dp, _dp]
+        L.orc_scalar_assemble.argtypes = [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, _dp, _dp, _dp, _dp, _ip, _dp,
+                                          _dp, ct.c_int, ct.c_double, _dp, _dp, _dp, _dp]
         _lib = L
     return _lib
 
@@ -153,6 +156,29 @@ class Oracle:
         o = np.zeros(11)
         arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p)]
         lib().orc_patch_force(self._h, patch, sign, mu, *map(_d, arrs), _d(o))
+        return o
+
+    def scalar_gradient(self, bc_type, bc_value, phi) -> np.ndarray:
+        """libpoisson/libscalar LSQ gradient (3 x nCells)."""
+        g = np.zeros((3, self.n_cells))
+        bt = np.ascontiguousarray(bc_type, np.int32)
+        bv = np.ascontiguousarray(bc_value, np.float64)
+        ph = np.ascontiguousarray(phi, np.float64)
+        lib().orc_scalar_gradient(self._h, _i(bt), _d(bv), _d(ph), _d(g[0]), _d(g[1]), _d(g[2]))
+        return g
+
+    def scalar_assemble(self, transport, upwind, nonorth, gamma, src, bc_type, bc_value, grad, flux=None, sp=None,
+                        ref_cell=-1, ref_value=0.0) -> dict:
+        """Elliptic (transport=False) or transport system in face-coefficient form."""
+        C, I = self.n_cells, self.n_internal
+        o = dict(diag=np.zeros(C), a_pn=np.zeros(I), a_np=np.zeros(I), rhs=np.zeros(C))
+        f64 = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)  # noqa: E731
+        gm, fl, sr, spp, bv = f64(gamma), f64(flux), f64(src), f64(sp), f64(bc_value)
+        g = np.ascontiguousarray(np.asarray(grad, np.float64).reshape(-1))
+        bt = np.ascontiguousarray(bc_type, np.int32)
+        lib().orc_scalar_assemble(self._h, int(transport), int(upwind), int(nonorth), _d(gm), _d(fl), _d(sr), _d(spp),
+                                  _i(bt), _d(bv), _d(g), int(ref_cell), float(ref_value), _d(o["diag"]),
+                                  _d(o["a_pn"]), _d(o["a_np"]), _d(o["rhs"]))
         return o
 
     def __del__(self):

@@ -3,6 +3,7 @@
   liboracle.so      oracle.cpp, the CPU restatement of the reference's SIMPLE iteration
   _ref/libgsv1ref.so the reference's own host code compiled from /root/reference where it lies
                      (only when that tree exists; see build_ref.sh for the recipe)
+  _ref/libscalarref.so the reference's libpoisson / libscalar host assembly, same recipe
 
 Usage: python -m oracle.build
 """
@@ -34,8 +35,11 @@ def build_ref(force: bool = False) -> Path | None:
     if not REFERENCE.exists():
         return out if out.exists() else None
     script = HERE / "build_ref.sh"
-    deps = [script, HERE / "ref_shim.cu", *sorted((HERE / "ref_stubs").iterdir())]
-    if force or not out.exists() or out.stat().st_mtime < max(d.stat().st_mtime for d in deps):
+    deps = [script, HERE / "ref_shim.cu", HERE / "ref_scalar_shim.cu", HERE / "ref_transport_shim.cu",
+            *sorted((HERE / "ref_stubs").iterdir())]
+    outs = [out, HERE / "_ref" / "libscalarref.so"]
+    newest = max(d.stat().st_mtime for d in deps)
+    if force or any(not o.exists() or o.stat().st_mtime < newest for o in outs):
         r = subprocess.run(["bash", str(script)], capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("reference build failed:\n" + r.stdout + r.stderr)

@@ -966,4 +966,129 @@ void orc_patch_force(const orc_mesh* m, int patch, int sign, double mu, const do
   (void)minD; (void)maxD; (void)maxUt; (void)maxSh;
 }
 
+/* ---- scalar libraries (libpoisson, libscalar) ------------------------------------------------
+ * bc_type per face (boundary entries read): 0 Dirichlet, 1 prescribed normal gradient, 2 zero
+ * gradient (libscalar). */
+
+/* compute_lsq_gradient of libpoisson/src/gradient.cu:21-83 (libscalar's copy at
+ * scalar_transport_library.cu:185-246 is the same): neighbours as usual, Dirichlet faces at the
+ * face centre, other boundary faces as the pure-normal constraint r = dn n, dphi = g dn. */
+void orc_scalar_gradient(const orc_mesh* m, const int* bt, const double* bv, const double* phi, double* gx,
+                         double* gy, double* gz) {
+#pragma omp parallel for schedule(static)
+  for (int P = 0; P < m->nCells; ++P) {
+    const V3 xP = m->cc[P];
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, b[3] = {0, 0, 0};
+    auto acc = [&](const V3& r, double dphi) {
+      const double w = 1.0 / std::max(dot3(r, r), 1e-30);
+      for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) M[i][j] += w * r[i] * r[j];
+        b[i] += w * r[i] * dphi;
+      }
+    };
+    for (int N : m->cellNbrs[P]) acc(sub3(m->cc[N], xP), phi[N] - phi[P]);
+    for (int f : m->cellBFace[P]) {
+      const V3 rcf = sub3(m->xf[f], xP);
+      if (bt[f] == 0) {
+        acc(rcf, bv[f] - phi[P]);
+      } else {
+        const double dn = std::max(dot3(rcf, m->nf[f]), 1e-30);
+        acc(mul3(dn, m->nf[f]), bv[f] * dn);
+      }
+    }
+    const double a = M[0][0], bb = M[0][1], c = M[0][2], d = M[1][0], e = M[1][1], f2 = M[1][2], g = M[2][0],
+                 h = M[2][1], k = M[2][2];
+    const double det = a * (e * k - f2 * h) - bb * (d * k - f2 * g) + c * (d * h - e * g);
+    double o[3] = {0, 0, 0};
+    if (std::fabs(det) > 1e-20) {
+      const double inv[3][3] = {{(e * k - f2 * h) / det, (c * h - bb * k) / det, (bb * f2 - c * e) / det},
+                                {(f2 * g - d * k) / det, (a * k - c * g) / det, (c * d - a * f2) / det},
+                                {(d * h - e * g) / det, (bb * g - a * h) / det, (a * e - bb * d) / det}};
+      for (int i = 0; i < 3; ++i) o[i] = inv[i][0] * b[0] + inv[i][1] * b[1] + inv[i][2] * b[2];
+    }
+    gx[P] = o[0];
+    gy[P] = o[1];
+    gz[P] = o[2];
+  }
+}
+
+/* Assembly in face-coefficient form: diag[C], a_pn[Fi] (row owner, column neighbour),
+ * a_np[Fi] (row neighbour, column owner), rhs[C].  transport == 0: libpoisson
+ * assemble_scalar_elliptic_system (scalar_elliptic.cu:60-136, reference cell row replaced by the
+ * identity as at 126-135); transport == 1: libscalar assemble_scalar_transport_system
+ * (scalar_transport_library.cu:250-357).  grad is 3 x nCells SoA; flux/sp may be NULL. */
+void orc_scalar_assemble(const orc_mesh* m, int transport, int upwind, int nonorth, const double* gamma,
+                         const double* flux, const double* src, const double* sp, const int* bt, const double* bv,
+                         const double* grad, int ref_cell, double ref_value, double* diag, double* a_pn,
+                         double* a_np, double* rhs) {
+  const int C = m->nCells, nI = m->nInternal;
+  const double *gx = grad, *gy = grad + C, *gz = grad + 2 * C;
+  for (int c = 0; c < C; ++c) {
+    rhs[c] = src[c] * m->vol[c];
+    diag[c] = (transport && sp) ? -sp[c] * m->vol[c] : 0.0;
+  }
+  for (int f = 0; f < nI; ++f) {
+    const int P = m->owner[f], N = m->neigh[f];
+    const V3 d = sub3(m->cc[N], m->cc[P]);
+    const double D = gamma[f] * dot3(m->Sf[f], m->Sf[f]) / std::max(dot3(d, m->Sf[f]), 1e-30);
+    diag[P] += D;
+    diag[N] += D;
+    a_pn[f] = -D;
+    a_np[f] = -D;
+    const V3 dx = sub3(m->xf[f], m->cc[P]);
+    const double lam = std::min(1.0, std::max(0.0, dot3(dx, d) / std::max(dot3(d, d), 1e-30)));
+    if (nonorth) {
+      const V3 T = sub3(m->Sf[f], mul3(D / std::max(gamma[f], 1e-30), d));
+      const V3 gf{(1.0 - lam) * gx[P] + lam * gx[N], (1.0 - lam) * gy[P] + lam * gy[N],
+                  (1.0 - lam) * gz[P] + lam * gz[N]};
+      const double corr = gamma[f] * dot3(T, gf);
+      rhs[P] += corr;
+      rhs[N] -= corr;
+    }
+    if (transport && flux) {
+      const double F = flux[f];
+      if (!upwind) {
+        diag[P] += F * (1.0 - lam);
+        a_pn[f] += F * lam;
+        a_np[f] -= F * (1.0 - lam);
+        diag[N] -= F * lam;
+      } else if (F >= 0.0) {
+        diag[P] += F;
+        a_np[f] -= F;
+      } else {
+        a_pn[f] += F;
+        diag[N] -= F;
+      }
+    }
+  }
+  for (int f = nI; f < m->nFaces; ++f) {
+    const int P = m->owner[f];
+    const V3 d = sub3(m->xf[f], m->cc[P]);
+    const double D = gamma[f] * dot3(m->Sf[f], m->Sf[f]) / std::max(dot3(d, m->Sf[f]), 1e-30);
+    const double F = (transport && flux) ? flux[f] : 0.0;
+    if (bt[f] == 0) {
+      diag[P] += D;
+      rhs[P] += D * bv[f];
+      if (nonorth) {
+        const V3 T = sub3(m->Sf[f], mul3(D / std::max(gamma[f], 1e-30), d));
+        rhs[P] += gamma[f] * (T[0] * gx[P] + T[1] * gy[P] + T[2] * gz[P]);
+      }
+      if (transport) rhs[P] += -F * bv[f];
+    } else if (transport) {
+      rhs[P] += gamma[f] * (bt[f] == 2 ? 0.0 : bv[f]) * m->Af[f];
+      diag[P] += F;
+    } else {
+      rhs[P] += -gamma[f] * bv[f] * m->Af[f];
+    }
+  }
+  if (ref_cell >= 0 && ref_cell < C) {
+    for (int f = 0; f < nI; ++f) {
+      if (m->owner[f] == ref_cell) a_pn[f] = 0.0;
+      if (m->neigh[f] == ref_cell) a_np[f] = 0.0;
+    }
+    diag[ref_cell] = 1.0;
+    rhs[ref_cell] = ref_value;
+  }
+}
+
 }  // extern "C"

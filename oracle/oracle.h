@@ -81,6 +81,16 @@ int orc_simple_run(orc_mesh* m, const orc_params* prm, int nsteps, double* u, do
 void orc_patch_force(const orc_mesh* m, int patch, int normal_sign, double mu, const double* u,
                      const double* v, const double* w, const double* p, double* out11);
 
+/* scalar libraries: libpoisson gradient (gradient.cu:21-83) and the elliptic / transport
+ * assemblies (scalar_elliptic.cu:60-136, scalar_transport_library.cu:250-357) in face-coefficient
+ * form; bc_type per face: 0 Dirichlet, 1 normal gradient, 2 zero gradient */
+void orc_scalar_gradient(const orc_mesh* m, const int* bc_type, const double* bc_value, const double* phi,
+                         double* gx, double* gy, double* gz);
+void orc_scalar_assemble(const orc_mesh* m, int transport, int upwind, int nonorth, const double* gamma,
+                         const double* flux, const double* src, const double* sp, const int* bc_type,
+                         const double* bc_value, const double* grad, int ref_cell, double ref_value,
+                         double* diag, double* a_pn, double* a_np, double* rhs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,6 +51,7 @@ HYPRE_Int HYPRE_IJMatrixCreate(MPI_Comm, HYPRE_BigInt, HYPRE_BigInt, HYPRE_BigIn
 HYPRE_Int HYPRE_IJMatrixSetObjectType(HYPRE_IJMatrix, HYPRE_Int);
 HYPRE_Int HYPRE_IJMatrixSetRowSizes(HYPRE_IJMatrix, const HYPRE_Int*);
 HYPRE_Int HYPRE_IJMatrixInitialize_v2(HYPRE_IJMatrix, HYPRE_MemoryLocation);
+HYPRE_Int HYPRE_IJMatrixInitialize(HYPRE_IJMatrix);
 HYPRE_Int HYPRE_IJMatrixSetValues(HYPRE_IJMatrix, HYPRE_Int, HYPRE_Int*, const HYPRE_BigInt*, const HYPRE_BigInt*, const HYPRE_Complex*);
 HYPRE_Int HYPRE_IJMatrixAssemble(HYPRE_IJMatrix);
 HYPRE_Int HYPRE_IJMatrixGetObject(HYPRE_IJMatrix, void**);
@@ -59,6 +60,7 @@ HYPRE_Int HYPRE_IJMatrixDestroy(HYPRE_IJMatrix);
 HYPRE_Int HYPRE_IJVectorCreate(MPI_Comm, HYPRE_BigInt, HYPRE_BigInt, HYPRE_IJVector*);
 HYPRE_Int HYPRE_IJVectorSetObjectType(HYPRE_IJVector, HYPRE_Int);
 HYPRE_Int HYPRE_IJVectorInitialize_v2(HYPRE_IJVector, HYPRE_MemoryLocation);
+HYPRE_Int HYPRE_IJVectorInitialize(HYPRE_IJVector);
 HYPRE_Int HYPRE_IJVectorSetValues(HYPRE_IJVector, HYPRE_Int, const HYPRE_BigInt*, const HYPRE_Complex*);
 HYPRE_Int HYPRE_IJVectorAssemble(HYPRE_IJVector);
 HYPRE_Int HYPRE_IJVectorMigrate(HYPRE_IJVector, HYPRE_MemoryLocation);

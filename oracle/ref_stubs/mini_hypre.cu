@@ -110,6 +110,7 @@ HYPRE_Int HYPRE_IJMatrixSetRowSizes(HYPRE_IJMatrix A, const HYPRE_Int* s) {
   return 0;
 }
 HYPRE_Int HYPRE_IJMatrixInitialize_v2(HYPRE_IJMatrix, HYPRE_MemoryLocation) { return 0; }
+HYPRE_Int HYPRE_IJMatrixInitialize(HYPRE_IJMatrix) { return 0; }
 HYPRE_Int HYPRE_IJMatrixSetValues(HYPRE_IJMatrix A, HYPRE_Int nrows, HYPRE_Int* ncols, const HYPRE_BigInt*,
                                   const HYPRE_BigInt* cols, const HYPRE_Complex* vals) {
   A->I.assign(nrows + 1, 0);
@@ -160,6 +161,7 @@ HYPRE_Int HYPRE_IJVectorCreate(MPI_Comm, HYPRE_BigInt il, HYPRE_BigInt iu, HYPRE
 }
 HYPRE_Int HYPRE_IJVectorSetObjectType(HYPRE_IJVector, HYPRE_Int) { return 0; }
 HYPRE_Int HYPRE_IJVectorInitialize_v2(HYPRE_IJVector, HYPRE_MemoryLocation) { return 0; }
+HYPRE_Int HYPRE_IJVectorInitialize(HYPRE_IJVector) { return 0; }
 HYPRE_Int HYPRE_IJVectorSetValues(HYPRE_IJVector v, HYPRE_Int n, const HYPRE_BigInt* idx, const HYPRE_Complex* x) {
   for (int k = 0; k < n; ++k) v->h[(size_t)idx[k]] = x[k];
   return 0;

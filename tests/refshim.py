@@ -141,3 +141,99 @@ def expand_case(argv: list[str]) -> list[str]:
     if n < 0:
         raise RuntimeError(err.value.decode())
     return out.raw.split(b"\0")[:n] and [s.decode() for s in out.raw.split(b"\0")[:n]]
+
+
+# ---- the reference's scalar libraries (oracle/_ref/libscalarref.so) ---------------------------
+SCALAR_LIB = LIB.parent / "libscalarref.so"
+_slib = None
+
+
+def scalar_available() -> bool:
+    return SCALAR_LIB.exists()
+
+
+def slib() -> ct.CDLL:
+    global _slib
+    if _slib is None:
+        L = ct.CDLL(str(SCALAR_LIB))
+        L.rsm_open.restype = ct.c_void_p
+        L.rsm_open.argtypes = [ct.c_char_p, ct.c_char_p, ct.c_int]
+        L.rsm_close.argtypes = [ct.c_void_p]
+        L.rsm_sizes.argtypes = [ct.c_void_p, _ip]
+        L.rsm_geometry.argtypes = [ct.c_void_p, _dp, _dp]
+        L.rsm_pattern.argtypes = [ct.c_void_p, _ip, _ip]
+        L.rst_pattern.argtypes = [ct.c_void_p, _ip, _ip]
+        L.rsm_poisson_gradient.argtypes = [ct.c_void_p, _ip, _dp, _dp, _dp]
+        L.rsm_poisson_assemble.restype = ct.c_int
+        L.rsm_poisson_assemble.argtypes = [ct.c_void_p, _dp, _dp, _ip, _dp, _dp, ct.c_int, ct.c_int, ct.c_int,
+                                           ct.c_double, _dp, _dp, ct.c_char_p, ct.c_int]
+        L.rst_gradient.argtypes = [ct.c_void_p, _ip, _dp, _dp, _dp]
+        L.rst_assemble.restype = ct.c_int
+        L.rst_assemble.argtypes = [ct.c_void_p, _dp, _dp, _dp, _dp, _ip, _dp, _dp, ct.c_int, ct.c_int, _dp, _dp,
+                                   ct.c_char_p, ct.c_int]
+        _slib = L
+    return _slib
+
+
+class RefScalar:
+    """libpoisson / libscalar host functions on a polyMesh read by libpoisson's reader; same
+    gradient/system interface as oracle.mms.OracleAssembler."""
+
+    def __init__(self, polymesh_dir):
+        err = ct.create_string_buffer(1024)
+        h = slib().rsm_open(str(polymesh_dir).encode(), err, 1024)
+        if not h:
+            raise RuntimeError(err.value.decode())
+        self._h = ct.c_void_p(h)
+        s = np.zeros(4, np.int32)
+        slib().rsm_sizes(self._h, _i(s))
+        self.n, self.n_faces, self.n_internal, self.nnz = map(int, s)
+        self.row_off = np.zeros(self.n + 1, np.int32)
+        self.cols = np.zeros(self.nnz, np.int32)
+        slib().rsm_pattern(self._h, _i(self.row_off), _i(self.cols))
+        self.cc = np.zeros(3 * self.n)
+        self.vol = np.zeros(self.n)
+        slib().rsm_geometry(self._h, _d(self.cc), _d(self.vol))
+
+    def transport_pattern(self):
+        ro = np.zeros(self.n + 1, np.int32)
+        co = np.zeros(self.nnz, np.int32)
+        slib().rst_pattern(self._h, _i(ro), _i(co))
+        return ro, co
+
+    def gradient(self, transport, bt, bv, phi):
+        g = np.zeros(3 * self.n)
+        bt = np.ascontiguousarray(bt, np.int32)
+        bv = np.ascontiguousarray(bv, np.float64)
+        ph = np.ascontiguousarray(phi, np.float64)
+        fn = slib().rst_gradient if transport else slib().rsm_poisson_gradient
+        fn(self._h, _i(bt), _d(bv), _d(ph), _d(g))
+        return g.reshape(3, self.n)
+
+    def system(self, transport, upwind, nonorth, gamma, src, sp, flux, bt, bv, grad, ref_cell, ref_value):
+        import scipy.sparse as sps
+
+        vals = np.zeros(self.nnz)
+        rhs = np.zeros(self.n)
+        err = ct.create_string_buffer(1024)
+        f64 = lambda a, n: np.zeros(n) if a is None else np.ascontiguousarray(a, np.float64)  # noqa: E731
+        g = np.ascontiguousarray(np.asarray(grad, np.float64).reshape(-1))
+        bt = np.ascontiguousarray(bt, np.int32)
+        bv = np.ascontiguousarray(bv, np.float64)
+        gm = f64(gamma, self.n_faces)
+        if transport:
+            rc = slib().rst_assemble(self._h, _d(f64(flux, self.n_faces)), _d(gm), _d(f64(src, self.n)),
+                                     _d(f64(sp, self.n)), _i(bt), _d(bv), _d(g), int(upwind), int(nonorth),
+                                     _d(vals), _d(rhs), err, 1024)
+        else:
+            rc = slib().rsm_poisson_assemble(self._h, _d(gm), _d(f64(src, self.n)), _i(bt), _d(bv), _d(g),
+                                             int(nonorth), int(ref_cell >= 0), max(ref_cell, 0), float(ref_value),
+                                             _d(vals), _d(rhs), err, 1024)
+        if rc:
+            raise RuntimeError(err.value.decode())
+        return sps.csr_matrix((vals, self.cols, self.row_off), shape=(self.n, self.n)), rhs
+
+    def __del__(self):
+        if getattr(self, "_h", None) is not None and _slib is not None:
+            _slib.rsm_close(self._h)
+            self._h = None
