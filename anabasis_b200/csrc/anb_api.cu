@@ -111,6 +111,14 @@ struct anb_ctx {
   // measurement
   Prof prof;
   AlgoBytes ab;
+  // mixed precision (precision == ANB_PRECISION_MIXED): float matrices and inner-solver vectors
+  bool mixed = false;
+  float *mval32 = nullptr, *mdiag32 = nullptr, *pval32 = nullptr, *pdiag32 = nullptr, *pwdinv32 = nullptr;
+  float* bw32[8] = {nullptr};
+  float *r32 = nullptr, *dx32 = nullptr;                     // 3*nCells each
+  float *pr32 = nullptr, *pz32 = nullptr, *pp0_32 = nullptr, *pp1_32 = nullptr, *pq32 = nullptr;
+  AmgDevT<float> amg32;
+  double innerRtol = 1e-4;    // relative reduction asked of one FP32 inner solve at most
   // scalar-library solves (allocated on first use)
   DevArena scalarArena;
   double *sMinv = nullptr, *sBcVal = nullptr, *sGamma = nullptr, *sFlux = nullptr, *sSrc = nullptr,
@@ -232,7 +240,11 @@ void poll(anb_ctx* c, const int* dflags, int count) {
 
 // Momentum: nc-component BiCGSTAB + Jacobi on the shared matrix; comps with active[q]==0 are
 // frozen.  Returns per-component iterations and convergence.
+void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3]);
+void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv);
+
 void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
+  if (c->mixed) return solve_momentum_mixed(c, active, its, conv);
   BicgArgs a{};
   a.A = mom_sell(c);
   a.nc = 3;
@@ -306,6 +318,7 @@ PcgArgs pcg_args(anb_ctx* c, const double* b, double* x, double rtol) {
 
 // Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
 void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  if (c->mixed) return solve_pressure_mixed(c, b, x, rtol, its, conv);
   PcgArgs a = pcg_args(c, b, x, rtol);
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
   if (amg) c->amg.lv[0].b = c->pr;
@@ -331,67 +344,272 @@ void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* it
   }
 }
 
-void ensure_amg(anb_ctx* c) {
-  if (!c->prm.p_use_amg) return;
-  if (!c->amgBuilt) {
-    std::vector<double> hv(c->nEnt), hd(c->C);
-    CK(cudaMemcpyAsync(hv.data(), c->pval, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(hd.data(), c->pdiag, hd.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    AmgSetupOptions opt;
-    c->amgHost = build_amg_hierarchy(c->L, hv, hd, opt);
-    AmgDev& A = c->amg;
-    A.nLevels = (int)c->amgHost.size();
-    DevArena& ar = c->amgArena;
-    for (int l = 0; l < A.nLevels; ++l) {
-      const AmgLevelHost& h = c->amgHost[l];
-      AmgLevelDev& d = A.lv[l];
-      d = AmgLevelDev{};
-      d.n = h.n;
-      d.nc = h.nc;
-      if (l == 0) {
-        d.sliceOff = c->dm.sliceOff;
-        d.col = c->dm.col;
-        d.val = c->pval;
-        d.diag = c->pdiag;
-        d.wdinv = c->pwdinv;
-      } else {
-        d.rowOff = ar.upload(h.rowOff);
-        d.col = ar.upload(h.col);
-        d.val = ar.alloc<double>(h.rowOff.back());
-        d.diag = ar.alloc<double>(h.n);
-        d.b = ar.alloc<double>(h.n);
-        d.wdinv = ar.alloc<double>(h.n);
-      }
-      d.x = ar.alloc<double>(h.n);
-      d.x2 = ar.alloc<double>(h.n);
-      if (l + 1 < A.nLevels) {
-        d.agg = ar.upload(h.agg);
-        d.memOff = ar.upload(h.memOff);
-        d.mem = ar.upload(h.mem);
-        d.gOff = ar.upload(h.gOff);
-        d.gIdx = ar.upload(h.gIdx);
-        d.nEntNext = c->amgHost[l + 1].rowOff.back();
-      }
+PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, double rtol) {
+  PcgArgsT<float> a{};
+  a.A = DSellT<float>{c->C, c->dm.sliceOff, c->dm.col, c->pval32, c->pdiag32};
+  a.b = b;
+  a.x = x;
+  a.r = c->pr32; a.z = c->pz32; a.p0 = c->pp0_32; a.p1 = c->pp1_32; a.q = c->pq32;
+  a.sc = c->scal + kScalPcg;
+  a.fl = c->flags + kFlagPcg;
+  a.atol = atol;
+  a.rtol = rtol;
+  a.maxit = c->prm.p_maxit;
+  a.red = c->red;
+  return a;
+}
+
+// Aggregation hierarchy for the current level-0 matrix (val0/diag0 on the device, storage type T),
+// coarse levels in T, coarsest inverse in double; the V-cycle is captured as a graph for `ga`.
+template <class T>
+void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const PcgArgsT<T>& ga) {
+  std::vector<T> hv(c->nEnt), hd(c->C);
+  CK(cudaMemcpyAsync(hv.data(), val0, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(hd.data(), diag0, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  AmgSetupOptions opt;
+  c->amgHost = build_amg_hierarchy(c->L, std::vector<double>(hv.begin(), hv.end()),
+                                   std::vector<double>(hd.begin(), hd.end()), opt);
+  A.nLevels = (int)c->amgHost.size();
+  DevArena& ar = c->amgArena;
+  for (int l = 0; l < A.nLevels; ++l) {
+    const AmgLevelHost& h = c->amgHost[l];
+    AmgLevelDevT<T>& d = A.lv[l];
+    d = AmgLevelDevT<T>{};
+    d.n = h.n;
+    d.nc = h.nc;
+    if (l == 0) {
+      d.sliceOff = c->dm.sliceOff;
+      d.col = c->dm.col;
+      d.val = val0;
+      d.diag = diag0;
+      d.wdinv = wdinv0;
+    } else {
+      d.rowOff = ar.upload(h.rowOff);
+      d.col = ar.upload(h.col);
+      d.val = ar.alloc<T>(h.rowOff.back());
+      d.diag = ar.alloc<T>(h.n);
+      d.b = ar.alloc<T>(h.n);
+      d.wdinv = ar.alloc<T>(h.n);
     }
-    const int nd = c->amgHost.back().n;
-    if (nd > 160) throw AnbError(ANB_ERR_UNSUPPORTED, "AMG coarsest level too large (" + std::to_string(nd) + ")");
-    A.nDense = nd;
-    A.dense = ar.alloc<double>((size_t)nd * nd);
-    c->amgBuilt = true;
-    const char* noGraph = std::getenv("ANB_NO_GRAPH");
-    if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) {
-      A.lv[0].b = c->pr;
-      CK(amg_capture_graph(c->lc, pcg_args(c, c->pb, c->Pc, 0.0), A));
+    d.x = ar.alloc<T>(h.n);
+    d.x2 = ar.alloc<T>(h.n);
+    if (l + 1 < A.nLevels) {
+      d.agg = ar.upload(h.agg);
+      d.memOff = ar.upload(h.memOff);
+      d.mem = ar.upload(h.mem);
+      d.gOff = ar.upload(h.gOff);
+      d.gIdx = ar.upload(h.gIdx);
+      d.nEntNext = c->amgHost[l + 1].rowOff.back();
     }
   }
+  const int nd = c->amgHost.back().n;
+  if (nd > 160) throw AnbError(ANB_ERR_UNSUPPORTED, "AMG coarsest level too large (" + std::to_string(nd) + ")");
+  A.nDense = nd;
+  A.dense = ar.alloc<double>((size_t)nd * nd);
+  c->amgBuilt = true;
+  const char* noGraph = std::getenv("ANB_NO_GRAPH");
+  if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) {
+    A.lv[0].b = ga.r;
+    CK(amg_capture_graph(c->lc, ga, A));
+  }
+}
+
+void ensure_amg(anb_ctx* c) {
+  if (!c->prm.p_use_amg) return;
+  if (c->mixed) {
+    if (!c->amgBuilt)
+      build_amg<float>(c, c->amg32, c->pval32, c->pdiag32, c->pwdinv32, pcg_args32(c, c->r32, c->dx32, 0.0, 0.0));
+    if (c->amg32.nLevels >= 2) amg_refresh(c->lc, c->amg32);
+    return;
+  }
+  if (!c->amgBuilt) build_amg<double>(c, c->amg, c->pval, c->pdiag, c->pwdinv, pcg_args(c, c->pb, c->Pc, 0.0));
   if (c->amg.nLevels >= 2) amg_refresh(c->lc, c->amg);
+}
+
+constexpr int kScalDefect = 32;  // 3 * 8
+constexpr int kFlagDefect = 16;  // 3 * 4
+constexpr int kFlagFrozen = 28;  // 3
+
+// Mixed precision: FP64 defect correction around FP32 inner solves.  Each sweep forms the FP64
+// residual r = b - A x with the float matrix and stops once |r| <= target = max(atol, rtol |b|);
+// otherwise it solves A dx = r in FP32, down to half the target or to a relative reduction
+// innerRtol, whichever is reached first (FP32 resolves about six digits of r), and adds dx to x.
+// Returns per-component inner iterations and convergence.
+void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
+  const int C = c->C;
+  DefectArgs d{};
+  d.A = DSellT<float>{C, c->dm.sliceOff, c->dm.col, c->mval32, c->mdiag32};
+  d.nc = 3;
+  d.b = c->rhs;
+  d.x = c->Us;
+  d.r32 = c->r32;
+  d.sc = c->scal + kScalDefect;
+  d.fl = c->flags + kFlagDefect;
+  d.frozen = c->flags + kFlagFrozen;
+  d.atol = c->prm.vel_tol;
+  d.rtol = c->prm.vel_rel_tol;
+  d.red = c->red;
+  const int fr[3] = {!active[0], !active[1], !active[2]};
+  CK(cudaMemcpyAsync(c->flags + kFlagFrozen, fr, sizeof(fr), cudaMemcpyHostToDevice, c->stream));
+  BicgArgsT<float> a{};
+  a.A = d.A;
+  a.nc = 3;
+  a.b = c->r32;
+  a.x = c->dx32;
+  a.r = c->bw32[0]; a.rh = c->bw32[1]; a.p = c->bw32[2]; a.v = c->bw32[3];
+  a.s = c->bw32[4]; a.t = c->bw32[5]; a.ph = c->bw32[6]; a.sh = c->bw32[7];
+  a.sc = c->scal + kScalBicg;
+  a.fl = c->flags + kFlagBicg;
+  a.rtol = c->innerRtol;
+  a.maxit = c->prm.vel_maxit;
+  a.red = c->red;
+  int tot[3] = {0, 0, 0};
+  bool outerConv[3] = {false, false, false};
+  for (int sweep = 0;; ++sweep) {
+    launch_defect(c->lc, d);
+    CK(cudaMemcpyAsync(c->hScal, d.sc, sizeof(double) * 24, cudaMemcpyDeviceToHost, c->stream));
+    poll(c, d.fl, 12);
+    bool all = true;
+    int innerFlags[12];
+    double target = 1e300;
+    for (int q = 0; q < 3; ++q) {
+      outerConv[q] = c->hFlags[4 * q] != 0;
+      all = all && outerConv[q];
+      // converged (or frozen) components sit out the inner solve
+      innerFlags[4 * q] = outerConv[q] ? 1 : 0;
+      innerFlags[4 * q + 1] = 0;
+      innerFlags[4 * q + 2] = 0;
+      innerFlags[4 * q + 3] = outerConv[q] ? 1 : 0;
+      if (!outerConv[q])
+        target = std::min(target, std::max(d.atol, d.rtol * std::sqrt(c->hScal[8 * q + 1])));
+    }
+    const bool budget = tot[0] < a.maxit && tot[1] < a.maxit && tot[2] < a.maxit;
+    if (all || !budget || sweep >= 50) break;
+    a.atol = 0.5 * target;
+    bicg_init(c->lc, a);
+    CK(cudaMemcpyAsync(a.fl, innerFlags, sizeof(innerFlags), cudaMemcpyHostToDevice, c->stream));
+    int done = 0;
+    int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
+    while (true) {
+      for (int k = 0; k < batch; ++k) bicg_iteration(c->lc, a);
+      done += batch;
+      poll(c, a.fl, 12);
+      bool fin = true;
+      for (int q = 0; q < 3; ++q) fin = fin && c->hFlags[4 * q];
+      if (fin || done > a.maxit + 2) break;
+      batch = 2;
+    }
+    int mx = 0;
+    for (int q = 0; q < 3; ++q) {
+      tot[q] += c->hFlags[4 * q + 2];
+      mx = std::max(mx, c->hFlags[4 * q + 2]);
+    }
+    c->lastMomIts = std::max(1, mx);
+    launch_apply_correction(c->lc, C, 3, c->Us, c->dx32);
+  }
+  for (int q = 0; q < 3; ++q) {
+    its[q] = active[q] ? tot[q] : 0;
+    conv[q] = active[q] ? outerConv[q] : true;
+  }
+}
+
+void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  DefectArgs d{};
+  d.A = DSellT<float>{c->C, c->dm.sliceOff, c->dm.col, c->pval32, c->pdiag32};
+  d.nc = 1;
+  d.b = b;
+  d.x = x;
+  d.r32 = c->r32;
+  d.sc = c->scal + kScalDefect;
+  d.fl = c->flags + kFlagDefect;
+  d.frozen = nullptr;
+  d.atol = c->prm.p_tol;
+  d.rtol = rtol;
+  d.red = c->red;
+  const AmgDevT<float>* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg32.nLevels >= 2) ? &c->amg32 : nullptr;
+  if (amg) c->amg32.lv[0].b = c->pr32;
+  int tot = 0;
+  bool ok = false;
+  for (int sweep = 0;; ++sweep) {
+    launch_defect(c->lc, d);
+    CK(cudaMemcpyAsync(c->hScal, d.sc, sizeof(double) * 2, cudaMemcpyDeviceToHost, c->stream));
+    poll(c, d.fl, 1);
+    ok = c->hFlags[0] != 0;
+    if (ok || tot >= c->prm.p_maxit || sweep >= 50) break;
+    const double target = std::max(d.atol, rtol * std::sqrt(c->hScal[1]));
+    PcgArgsT<float> a = pcg_args32(c, c->r32, c->dx32, 0.5 * target, c->innerRtol);
+    pcg_init(c->lc, a);
+    pcg_precondition(c->lc, a, amg);
+    int it = 0;
+    int batch = std::max(2, std::min(3 * c->lastPIts / 4, 64));
+    const int tail = std::max(2, c->lastPIts / 8);
+    while (true) {
+      for (int k = 0; k < batch; ++k) pcg_iteration(c->lc, a, it++, amg);
+      poll(c, a.fl, 4);
+      if (c->hFlags[0] || it > a.maxit + 2) break;
+      batch = tail;
+    }
+    const int n = c->hFlags[1];
+    tot += n;
+    c->lastPIts = std::max(1, n);
+    if (c->prof.family == kKfPcgSpmv) {  // launches after convergence returned at once
+      c->prof.bytes -= (double)(it - n) * (20.0 * c->ab.C + 8.0 * c->ab.nnzOff);
+      c->prof.launches -= it - n;
+    }
+    launch_apply_correction(c->lc, c->C, 1, x, c->dx32);
+  }
+  *its = tot;
+  *conv = ok;
 }
 
 void check_ready(anb_ctx* c) {
   if (!c->bcSet) throw AnbError(ANB_ERR_INVALID, "boundary conditions not set (anb_set_bc)");
   if (!c->stateSet) throw AnbError(ANB_ERR_INVALID, "state not set (anb_set_state)");
   CK(cudaSetDevice(c->prm.device));
+}
+
+// Momentum assembly into the matrix storage of the context's precision; Q is the field of the
+// relaxation term (the old velocity, or the current iterate for rhs-only re-assembly).
+template <class M>
+void launch_mom_t(anb_ctx* c, M* val, M* diag, const double* Q, int rhsOnly) {
+  MomArgsT<M> ma{};
+  ma.U = c->U;
+  ma.Q = Q;
+  ma.G = c->G;
+  ma.rho = c->prm.rho;
+  ma.mu = c->prm.mu;
+  ma.uRelax = c->prm.u_relax;
+  ma.relax = c->prm.u_relax < 0.999999 ? 1 : 0;
+  ma.rhsOnly = rhsOnly;
+  ma.val = val;
+  ma.diag = diag;
+  ma.rhs = c->rhs;
+  ma.rau = c->rau;
+  launch_momentum(c->lc, c->dm, ma);
+}
+void launch_mom(anb_ctx* c, const double* Q, int rhsOnly) {
+  if (c->mixed) launch_mom_t<float>(c, c->mval32, c->mdiag32, Q, rhsOnly);
+  else launch_mom_t<double>(c, c->mval, c->mdiag, Q, rhsOnly);
+}
+
+template <class M>
+void launch_prc(anb_ctx* c, M* val, M* diag, M* wdinv) {
+  PresArgsT<M> pa{};
+  pa.Us = c->Us;
+  pa.P = c->P;
+  pa.Gp = c->G + 9 * (size_t)c->C;
+  pa.rau = c->rau;
+  pa.rho = c->prm.rho;
+  pa.val = val;
+  pa.diag = diag;
+  pa.phiStar = c->phiStar;
+  pa.divStar = c->divStar;
+  pa.b = c->pb;
+  pa.pc = c->Pc;
+  pa.wdinv = wdinv;
+  pa.omega = c->amg.omega;
+  launch_pressure_rc(c->lc, c->dm, pa);
 }
 
 // One SIMPLE outer iteration, main.cu:3388-3634.
@@ -412,20 +630,7 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
     grad(c, 4, phi, bits, out);
   }
   // 2. momentum matrix (u pass) + three right-hand sides + relaxation + rAU
-  MomArgs ma{};
-  ma.U = c->U;
-  ma.Q = c->U;
-  ma.G = c->G;
-  ma.rho = p.rho;
-  ma.mu = p.mu;
-  ma.uRelax = p.u_relax;
-  ma.relax = p.u_relax < 0.999999 ? 1 : 0;
-  ma.rhsOnly = 0;
-  ma.val = c->mval;
-  ma.diag = c->mdiag;
-  ma.rhs = c->rhs;
-  ma.rau = c->rau;
-  launch_momentum(c->lc, c->dm, ma);
+  launch_mom(c, c->U, 0);
   CK(cudaMemcpyAsync(c->Us, c->U, sizeof(double) * 3 * C, cudaMemcpyDeviceToDevice, c->stream));
   int its[3] = {0, 0, 0};
   {
@@ -439,10 +644,7 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
         const unsigned char bits[3] = {1, 2, 4};
         double* out[3] = {c->G, c->G + 3 * C, c->G + 6 * C};
         grad(c, 3, phi, bits, out);
-        MomArgs mr = ma;
-        mr.Q = c->Us;
-        mr.rhsOnly = 1;
-        launch_momentum(c->lc, c->dm, mr);
+        launch_mom(c, c->Us, 1);
       }
       // keep the iterate for the relative-change test (main.cu:3377-3381)
       std::vector<double> before;
@@ -477,21 +679,8 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
     }
   }
   // 3. pressure matrix + Rhie-Chow flux + continuity, p' = 0
-  PresArgs pa{};
-  pa.Us = c->Us;
-  pa.P = c->P;
-  pa.Gp = c->G + 9 * C;
-  pa.rau = c->rau;
-  pa.rho = p.rho;
-  pa.val = c->pval;
-  pa.diag = c->pdiag;
-  pa.phiStar = c->phiStar;
-  pa.divStar = c->divStar;
-  pa.b = c->pb;
-  pa.pc = c->Pc;
-  pa.wdinv = c->pwdinv;
-  pa.omega = c->amg.omega;
-  launch_pressure_rc(c->lc, c->dm, pa);
+  if (c->mixed) launch_prc<float>(c, c->pval32, c->pdiag32, c->pwdinv32);
+  else launch_prc<double>(c, c->pval, c->pdiag, c->pwdinv);
   const int every = std::max(p.p_amg_rebuild_every, 1);
   if (!c->amgBuilt || c->outerStep == 1 || ((c->outerStep - 1) % every) == 0) ensure_amg(c);
   // 4. non-orthogonal pressure passes
@@ -754,26 +943,51 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     c->rau = A.alloc<double>(C);
     c->G = A.alloc<double>(12 * C);
     c->Gc = A.alloc<double>(3 * C);
-    c->mval = A.alloc<double>(c->nEnt);
-    c->mdiag = A.alloc<double>(C);
+    c->mixed = prm->precision == ANB_PRECISION_MIXED;
+    if (!c->mixed) {
+      c->mval = A.alloc<double>(c->nEnt);
+      c->mdiag = A.alloc<double>(C);
+      c->pval = A.alloc<double>(c->nEnt);
+      c->pdiag = A.alloc<double>(C);
+    } else {
+      c->mval32 = A.alloc<float>(c->nEnt);
+      c->mdiag32 = A.alloc<float>(C);
+      c->pval32 = A.alloc<float>(c->nEnt);
+      c->pdiag32 = A.alloc<float>(C);
+      c->pwdinv32 = A.alloc<float>(C);
+      for (int k = 0; k < 8; ++k) c->bw32[k] = A.alloc<float>(3 * C);
+      c->r32 = A.alloc<float>(3 * C);
+      c->dx32 = A.alloc<float>(3 * C);
+      c->pr32 = A.alloc<float>(C);
+      c->pz32 = A.alloc<float>(C);
+      c->pp0_32 = A.alloc<float>(C);
+      c->pp1_32 = A.alloc<float>(C);
+      c->pq32 = A.alloc<float>(C);
+      CK(cudaMemset(c->mval32, 0, sizeof(float) * c->nEnt));
+      CK(cudaMemset(c->pval32, 0, sizeof(float) * c->nEnt));
+      CK(cudaMemset(c->dx32, 0, sizeof(float) * 3 * C));
+      if (const char* s = std::getenv("ANB_MIXED_INNER_RTOL")) c->innerRtol = std::atof(s);
+    }
     c->rhs = A.alloc<double>(3 * C);
-    c->pval = A.alloc<double>(c->nEnt);
-    c->pdiag = A.alloc<double>(C);
     c->pb = A.alloc<double>(C);
     c->divStar = A.alloc<double>(C);
     c->divCorr = A.alloc<double>(C);
     c->phiStar = A.alloc<double>(F);
     c->phi = A.alloc<double>(F);
-    for (int k = 0; k < 8; ++k) c->bw[k] = A.alloc<double>(3 * C);
-    c->pr = A.alloc<double>(C);
-    c->pz = A.alloc<double>(C);
-    c->pp0 = A.alloc<double>(C);
-    c->pp1 = A.alloc<double>(C);
-    c->pq = A.alloc<double>(C);
+    if (!c->mixed) {
+      for (int k = 0; k < 8; ++k) c->bw[k] = A.alloc<double>(3 * C);
+      c->pr = A.alloc<double>(C);
+      c->pz = A.alloc<double>(C);
+      c->pp0 = A.alloc<double>(C);
+      c->pp1 = A.alloc<double>(C);
+      c->pq = A.alloc<double>(C);
+      c->pwdinv = A.alloc<double>(C);
+    }
     c->pdx = A.alloc<double>(C);
-    c->pwdinv = A.alloc<double>(C);
     if (const char* s = std::getenv("ANB_AMG_OMEGA")) c->amg.omega = std::atof(s);
     if (const char* s = std::getenv("ANB_AMG_CORR")) c->amg.corr = std::atof(s);
+    c->amg32.omega = c->amg.omega;
+    c->amg32.corr = c->amg.corr;
     c->scal = A.alloc<double>(64);
     c->flags = A.alloc<int>(32);
     c->stats = A.alloc<double>(16);
@@ -781,8 +995,10 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     c->red.partials = A.alloc<double>((size_t)(nSM * 8 + 16) * 16);
     c->red.ticket = A.alloc<unsigned int>(1);
     CK(cudaMemset(c->red.ticket, 0, sizeof(unsigned int)));
-    CK(cudaMemset(c->mval, 0, sizeof(double) * c->nEnt));
-    CK(cudaMemset(c->pval, 0, sizeof(double) * c->nEnt));
+    if (!c->mixed) {
+      CK(cudaMemset(c->mval, 0, sizeof(double) * c->nEnt));
+      CK(cudaMemset(c->pval, 0, sizeof(double) * c->nEnt));
+    }
     CK(cudaMemset(c->phi, 0, sizeof(double) * F));
     CK(cudaMemset(c->Pc, 0, sizeof(double) * C));
     CK(cudaMallocHost(&c->hFlags, sizeof(int) * 32));
@@ -808,6 +1024,7 @@ void anb_destroy(anb_ctx* c) {
   cudaSetDevice(c->prm.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
+  if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
   c->amgArena.release();
   c->arena.release();
   if (c->hFlags) cudaFreeHost(c->hFlags);
@@ -960,6 +1177,11 @@ void release_amg(anb_ctx* c) {
   c->amg.graphKernels = 0;
   c->amg.nLevels = 0;
   c->amg.dense = nullptr;
+  if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
+  c->amg32.graph = nullptr;
+  c->amg32.graphKernels = 0;
+  c->amg32.nLevels = 0;
+  c->amg32.dense = nullptr;
   c->amgArena.release();
   c->amgHost.clear();
   c->amgBuilt = false;
@@ -1057,6 +1279,7 @@ int anb_scalar_elliptic_solve(anb_ctx* c, const double* gammaFace, const double*
                               anb_solve_info* info) {
   if (!c || !source || !bcType || !bcValue || !phi) return ANB_ERR_INVALID;
   return guarded(c, [&]() -> int {
+    if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "this entry point needs an FP64 (ANB_PRECISION_FP64) context");
     CK(cudaSetDevice(c->prm.device));
     if (info) std::memset(info, 0, sizeof(*info));
     bool anyDirichlet = false;
@@ -1133,6 +1356,7 @@ int anb_scalar_transport_solve(anb_ctx* c, const double* flux, const double* gam
   if (!c || !gammaFace || !su || !bcType || !bcValue || !phi) return ANB_ERR_INVALID;
   if (convection != ANB_CONVECTION_CENTRAL && convection != ANB_CONVECTION_UPWIND) return ANB_ERR_INVALID;
   return guarded(c, [&]() -> int {
+    if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "this entry point needs an FP64 (ANB_PRECISION_FP64) context");
     CK(cudaSetDevice(c->prm.device));
     if (info) std::memset(info, 0, sizeof(*info));
     ensure_scalar_buffers(c);
@@ -1246,6 +1470,7 @@ int anb_debug_momentum(anb_ctx* c, const double* u, const double* v, const doubl
   int rc = anb_set_state(c, u, v, w, p);
   if (rc) return rc;
   return guarded(c, [&]() -> int {
+    if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "this entry point needs an FP64 (ANB_PRECISION_FP64) context");
     check_ready(c);
     const int C = c->C;
     const double* phi[4] = {c->U, c->U + C, c->U + 2 * C, c->P};
@@ -1283,6 +1508,7 @@ int anb_debug_pressure(anb_ctx* c, const double* u, const double* v, const doubl
                        const double* rau, double* diag, double* a_pn, double* phi_star, double* div_star) {
   if (!c) return ANB_ERR_INVALID;
   return guarded(c, [&]() -> int {
+    if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "this entry point needs an FP64 (ANB_PRECISION_FP64) context");
     if (!c->bcSet) throw AnbError(ANB_ERR_INVALID, "boundary conditions not set");
     CK(cudaSetDevice(c->prm.device));
     const int C = c->C;
@@ -1325,6 +1551,7 @@ int anb_debug_pressure(anb_ctx* c, const double* u, const double* v, const doubl
 int anb_debug_pressure_solve(anb_ctx* c, const double* b, double* x, int* iters, double* final_res) {
   if (!c) return ANB_ERR_INVALID;
   return guarded(c, [&]() -> int {
+    if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "this entry point needs an FP64 (ANB_PRECISION_FP64) context");
     CK(cudaSetDevice(c->prm.device));
     const double* s1[1] = {b};
     upload_cells(c, s1, c->pb, 1);

@@ -95,36 +95,44 @@ struct GradArgs {
 };
 void launch_lsq_grad(const LaunchCfg& lc, const DMesh& m, const GradArgs& a);
 
-struct MomArgs {
+// M: storage type of the assembled matrix (double plain, float mixed precision); the right-hand
+// sides, rAU and all arithmetic stay double.
+template <class M>
+struct MomArgsT {
   const double* U;    // 3*nCells old velocity (convecting velocity)
   const double* Q;    // 3*nCells field of the relaxation term (old field, or current iterate)
   const double* G;    // gradients of Q: [grad q0 | grad q1 | grad q2 | grad p], each 3*nCells SoA
   double rho, mu, uRelax;
   int relax;
   int rhsOnly;        // 1: right-hand sides only, relaxation from the stored relaxed diagonal
-  double* val;
-  double* diag;
+  M* val;
+  M* diag;
   double* rhs;        // 3*nCells
   double* rau;
 };
-void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgs& a);
+using MomArgs = MomArgsT<double>;
+template <class M>
+void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgsT<M>& a);
 
-struct PresArgs {
+template <class M>
+struct PresArgsT {
   const double* Us;   // 3*nCells momentum solution
   const double* P;
   const double* Gp;   // 3*nCells SoA
   const double* rau;
   double rho;
-  double* val;
-  double* diag;
+  M* val;
+  M* diag;
   double* phiStar;    // nInternal + nBoundary
   double* divStar;
   double* b;          // first pressure right-hand side, -divStar
   double* pc;         // zeroed p'
-  double* wdinv;      // optional: omega / diag for the AMG smoother
+  M* wdinv;           // optional: omega / diag for the AMG smoother
   double omega;
 };
-void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgs& a);
+using PresArgs = PresArgsT<double>;
+template <class M>
+void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgsT<M>& a);
 
 // Scalar elliptic (libpoisson) and steady scalar transport (libscalar) systems on the SIMPLE
 // layout.  Face arrays: internal faces in layout order and orientation, then boundary faces.

@@ -69,7 +69,8 @@ __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
 
 // ---- momentum: K25,K4,K2,K3,K5,K6 + rhs-only K26,K9,K7,K8,K10 for V and W in one pass ------
 // main.cu:1678-1896 (assembly), 1686-1695 (relaxation), 1787-1802 (rAU), loop 3350-3405.
-__global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgs a) {
+template <class M>
+__global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
   const int C = m.nCells;
   const double* U0 = a.U;
   const double* U1 = a.U + C;
@@ -88,11 +89,11 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgs a) {
       const int e = base + (k << 5);
       const int f = __ldg(&m.slotFace[e]);
       if (f < 0) {
-        if (full) a.val[e] = 0.0;
+        if (full) a.val[e] = M(0);
         continue;
       }
       if (!(__ldg(&m.fFlags[f]) & 1)) {
-        if (full) a.val[e] = 0.0;
+        if (full) a.val[e] = M(0);
         continue;
       }
       const int c = __ldg(&m.col[e]);
@@ -114,11 +115,11 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgs a) {
         corr[q] = mu * (gx * t[0] + gy * t[1] + gz * t[2]);
       }
       if (own) {
-        if (full) a.val[e] = -alpha + F * lam;
+        if (full) a.val[e] = (M)(-alpha + F * lam);
         diag += alpha + F * l1;
         rhs0 += corr[0]; rhs1 += corr[1]; rhs2 += corr[2];
       } else {
-        if (full) a.val[e] = -alpha - F * l1;
+        if (full) a.val[e] = (M)(-alpha - F * l1);
         diag += alpha - F * lam;
         rhs0 -= corr[0]; rhs1 -= corr[1]; rhs2 -= corr[2];
       }
@@ -150,11 +151,11 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgs a) {
         rhs1 += (invR - 1.0) * aPold * q1;
         rhs2 += (invR - 1.0) * aPold * q2;
       }
-      a.diag[r] = diag;
+      a.diag[r] = (M)diag;
       a.rau[r] = fabs(diag) > 1e-30 ? V / diag : 0.0;
     } else if (a.relax) {                                 // K10 for every re-solve
       const double invR = 1.0 / a.uRelax;
-      const double aPold = a.diag[r] * a.uRelax;
+      const double aPold = (double)a.diag[r] * a.uRelax;
       rhs0 += (invR - 1.0) * aPold * q0;
       rhs1 += (invR - 1.0) * aPold * q1;
       rhs2 += (invR - 1.0) * aPold * q2;
@@ -167,7 +168,8 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgs a) {
 
 // ---- pressure matrix (K11,K12) + Rhie-Chow flux (K14) + continuity (K15) ------------------
 // main.cu:1898-1950, 1474-1536, launch sequence 3407-3452.
-__global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgs a) {
+template <class M>
+__global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a) {
   const int C = m.nCells, nI = m.nInternal;
   const double* U0 = a.Us;
   const double* U1 = a.Us + C;
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgs a) {
       const int e = base + (k << 5);
       const int f = __ldg(&m.slotFace[e]);
       if (f < 0) {
-        a.val[e] = 0.0;
+        a.val[e] = M(0);
         continue;
       }
       const int c = __ldg(&m.col[e]);
@@ -195,10 +197,10 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgs a) {
       const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
       if (__ldg(&m.fFlags[f]) & 1) {
         const double coeff = g * rAUf;
-        a.val[e] = -coeff;
+        a.val[e] = (M)(-coeff);
         pd += coeff;
       } else {
-        a.val[e] = 0.0;
+        a.val[e] = M(0);
       }
       const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
       const double ub = l1 * U0[P] + lam * U0[N], vb = l1 * U1[P] + lam * U1[N], wb = l1 * U2[P] + lam * U2[N];
@@ -228,8 +230,8 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgs a) {
       div += phi;
       a.phiStar[nI + bf] = phi;
     }
-    a.diag[r] = pd;
-    if (a.wdinv) a.wdinv[r] = a.omega / pd;  // level-0 smoother weight, always from the current matrix
+    a.diag[r] = (M)pd;
+    if (a.wdinv) a.wdinv[r] = (M)(a.omega / pd);  // level-0 smoother weight, always from the current matrix
     a.divStar[r] = div;
     a.b[r] = -div;
     a.pc[r] = 0.0;
@@ -433,14 +435,20 @@ void launch_lsq_grad(const LaunchCfg& lc, const DMesh& m, const GradArgs& a) {
   else if (a.nf == 2) k_lsq_grad<2><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else k_lsq_grad<1><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
-void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgs& a) {
+template <class M>
+void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgsT<M>& a) {
   ProfScope ps(lc, kKfMomentum, lc.ab ? lc.ab->momentum() : 0.0);
-  k_momentum<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  k_momentum<M><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
-void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgs& a) {
+template <class M>
+void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgsT<M>& a) {
   ProfScope ps(lc, kKfPressureRc, lc.ab ? lc.ab->pressure_rc() : 0.0);
-  k_pressure_rc<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  k_pressure_rc<M><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
+template void launch_momentum<double>(const LaunchCfg&, const DMesh&, const MomArgsT<double>&);
+template void launch_momentum<float>(const LaunchCfg&, const DMesh&, const MomArgsT<float>&);
+template void launch_pressure_rc<double>(const LaunchCfg&, const DMesh&, const PresArgsT<double>&);
+template void launch_pressure_rc<float>(const LaunchCfg&, const DMesh&, const PresArgsT<float>&);
 void launch_nonorth_rhs(const LaunchCfg& lc, const DMesh& m, const NonOrthArgs& a) {
   ProfScope ps(lc, kKfNonOrth, lc.ab ? lc.ab->nonorth() : 0.0);
   k_nonorth_rhs<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
