@@ -60,6 +60,11 @@ class ForceReport(ct.Structure):
                 ("max_wall_distance", ct.c_double), ("max_ut", ct.c_double), ("max_shear_mag", ct.c_double)]
 
 
+class AdjointInfo(ct.Structure):
+    _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("res_norm", ct.c_double),
+                ("rhs_norm", ct.c_double), ("seconds", ct.c_double)]
+
+
 class SolveInfo(ct.Structure):
     _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("outer", ct.c_int),
                 ("final_res_norm", ct.c_double), ("final_rel_res", ct.c_double)]
@@ -79,6 +84,17 @@ SIGNATURES = {
     "anb_simple_iterate": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_double, ct.POINTER(IterStats), _ip]),
     "anb_patch_force": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
     "anb_patch_force_nalloc": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.POINTER(ForceReport)]),
+    "anb_set_viscosity": (ct.c_int, [ct.c_void_p, ct.c_double]),
+    "anb_steady_residual": (ct.c_int, [ct.c_void_p, _dp, _dp]),
+    "anb_force_objective": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _dp, _dp, _dp]),
+    "anb_newton_solve": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_int, _ip, _dp,
+                                    ct.POINTER(AdjointInfo)]),
+    "anb_tangent_linear": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _dp, _dp, ct.c_double, _dp,
+                                      ct.POINTER(AdjointInfo)]),
+    "anb_adjoint_force_grad": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, _dp, _dp, _dp, _dp,
+                                          ct.POINTER(AdjointInfo)]),
+    "anb_debug_jvp": (ct.c_int, [ct.c_void_p, _dp, _dp, ct.c_double, _dp]),
+    "anb_debug_vjp": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp]),
     "anb_scalar_elliptic_solve": (ct.c_int, [ct.c_void_p, _dp, _dp, _ip, _dp, ct.c_int, ct.c_int, ct.c_int, ct.c_int,
                                              ct.c_double, ct.c_double, ct.c_double, ct.c_int, _dp,
                                              ct.POINTER(SolveInfo)]),
@@ -298,6 +314,64 @@ class Solver:
                                                      rel_tol, max_iter, _d(x), _d(phi), ct.byref(info)),
                     ok=(ANB_OK, ANB_NOT_CONVERGED))
         return phi, dict((f, getattr(info, f)) for f, _ in SolveInfo._fields_)
+
+    # ---- steady sensitivities (include/anb.h) ----
+    def set_viscosity(self, mu: float) -> None:
+        self._check(lib().anb_set_viscosity(self._h, float(mu)))
+        self.params.mu = float(mu)
+
+    def steady_residual(self) -> tuple[np.ndarray, np.ndarray]:
+        r = np.zeros(4 * self.n_cells)
+        n = np.zeros(2)
+        self._check(lib().anb_steady_residual(self._h, _d(r), _d(n)))
+        return r, n
+
+    def force_objective(self, patch: int, direction=(1.0, 0.0, 0.0), normal_sign: int = -1) -> tuple[float, float]:
+        d = np.ascontiguousarray(direction, np.float64)
+        J, jm = ct.c_double(0), ct.c_double(0)
+        self._check(lib().anb_force_objective(self._h, patch, normal_sign, _d(d), ct.byref(J), ct.byref(jm)))
+        return J.value, jm.value
+
+    def newton_solve(self, max_newton=8, tol=1e-12, lin_max_iter=400) -> dict:
+        info = AdjointInfo()
+        steps, rn = ct.c_int(0), ct.c_double(0)
+        rc = lib().anb_newton_solve(self._h, max_newton, tol, lin_max_iter, ct.byref(steps), ct.byref(rn),
+                                    ct.byref(info))
+        self._check(rc, ok=(ANB_OK, ANB_NOT_CONVERGED))
+        return dict(steps=steps.value, res_norm=rn.value, converged=rc == ANB_OK, iterations=info.iterations,
+                    seconds=info.seconds)
+
+    def tangent_linear(self, patch, direction, dbc, dmu, normal_sign=-1) -> tuple[float, dict]:
+        d = np.ascontiguousarray(direction, np.float64)
+        b = np.ascontiguousarray(dbc, np.float64)
+        info = AdjointInfo()
+        dJ = ct.c_double(0)
+        self._check(lib().anb_tangent_linear(self._h, patch, normal_sign, _d(d), _d(b), float(dmu), ct.byref(dJ),
+                                             ct.byref(info)), ok=(ANB_OK, ANB_NOT_CONVERGED))
+        return dJ.value, dict((f, getattr(info, f)) for f, _ in AdjointInfo._fields_)
+
+    def adjoint_force_grad(self, patch, direction=(1.0, 0.0, 0.0), normal_sign=-1) -> tuple[np.ndarray, float, float, dict]:
+        d = np.ascontiguousarray(direction, np.float64)
+        g = np.zeros(3 * self.n_faces)
+        gm, J = ct.c_double(0), ct.c_double(0)
+        info = AdjointInfo()
+        self._check(lib().anb_adjoint_force_grad(self._h, patch, normal_sign, _d(d), _d(g), ct.byref(gm), ct.byref(J),
+                                                 ct.byref(info)), ok=(ANB_OK, ANB_NOT_CONVERGED))
+        return g, gm.value, J.value, dict((f, getattr(info, f)) for f, _ in AdjointInfo._fields_)
+
+    def debug_jvp(self, dX, dbc=None, dmu=0.0) -> np.ndarray:
+        out = np.zeros(4 * self.n_cells)
+        x = np.ascontiguousarray(dX, np.float64)
+        b = None if dbc is None else np.ascontiguousarray(dbc, np.float64)
+        self._check(lib().anb_debug_jvp(self._h, _d(x), _d(b), float(dmu), _d(out)))
+        return out
+
+    def debug_vjp(self, w) -> tuple[np.ndarray, np.ndarray, float]:
+        out = np.zeros(4 * self.n_cells)
+        g = np.zeros(3 * self.n_faces)
+        gm = np.zeros(1)
+        self._check(lib().anb_debug_vjp(self._h, _d(np.ascontiguousarray(w, np.float64)), _d(out), _d(g), _d(gm)))
+        return out, g, float(gm[0])
 
     def iterate(self, nsteps: int, tol_mass=-1.0, tol_vel=-1.0) -> tuple[int, list]:
         st = (IterStats * max(nsteps, 1))()

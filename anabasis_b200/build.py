@@ -25,7 +25,7 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["host_mesh.cpp", "host_case.cpp", "host_output.cpp", "host_api.cpp", "layout.cpp", "amg_setup.cpp"]
-CUDA_SOURCES = ["kernels_fv.cu", "kernels_krylov.cu", "kernels_scalar.cu", "anb_api.cu", "nalloc.cu"]
+CUDA_SOURCES = ["kernels_fv.cu", "kernels_krylov.cu", "kernels_scalar.cu", "kernels_adjoint.cu", "anb_api.cu", "adjoint_api.cu", "nalloc.cu"]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
 NVCCFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr"]
 

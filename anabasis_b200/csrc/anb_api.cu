@@ -9,124 +9,10 @@
 #include <string>
 #include <vector>
 
-#include "../../include/anb.h"
-#include "amg_setup.hpp"
+#include "context.hpp"
 #include "context_access.hpp"
-#include "host_mesh.hpp"
-#include "kernels.cuh"
-#include "layout.hpp"
 
 namespace anb {
-
-struct AnbError : std::runtime_error {
-  int code;
-  AnbError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define CK(call)                                                                                          \
-  do {                                                                                                    \
-    cudaError_t e_ = (call);                                                                              \
-    if (e_ != cudaSuccess)                                                                                \
-      throw AnbError(ANB_ERR_CUDA, std::string("CUDA error ") + cudaGetErrorString(e_) + " at " #call);   \
-  } while (0)
-
-// Device allocations owned by a context; freed together.
-class DevArena {
- public:
-  ~DevArena() { release(); }
-  template <class T>
-  T* alloc(size_t n) {
-    void* p = nullptr;
-    if (n == 0) n = 1;
-    CK(cudaMalloc(&p, n * sizeof(T)));
-    ptrs_.push_back(p);
-    bytes_ += n * sizeof(T);
-    return static_cast<T*>(p);
-  }
-  template <class T>
-  T* upload(const std::vector<T>& h) {
-    T* d = alloc<T>(h.size());
-    if (!h.empty()) CK(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
-    return d;
-  }
-  void release() {
-    for (void* p : ptrs_) cudaFree(p);
-    ptrs_.clear();
-    bytes_ = 0;
-  }
-  size_t bytes() const { return bytes_; }
-
- private:
-  std::vector<void*> ptrs_;
-  size_t bytes_ = 0;
-};
-
-}  // namespace anb
-
-using namespace anb;
-
-struct anb_ctx {
-  std::string err;
-  anb_params prm{};
-  HostMesh hm;
-  Layout L;
-  int C = 0, nI = 0, nB = 0, nEnt = 0;
-  cudaStream_t stream = nullptr;
-  LaunchCfg lc{};
-  DevArena arena, amgArena;
-  DMesh dm{};
-  // face-slot lookup for diagnostics: storage entry of (owner row, neighbour col) and back
-  std::vector<int> slotOwn, slotNei;
-  // device buffers
-  FaceRec* dFace = nullptr;
-  BndRec* dBnd = nullptr;
-  uint8_t* dBType = nullptr;
-  double* dBVal = nullptr;
-  double *dBA = nullptr, *dBN = nullptr;
-  double *U = nullptr, *Us = nullptr, *P = nullptr, *Pc = nullptr, *rau = nullptr;
-  double *G = nullptr, *Gc = nullptr;
-  double *mval = nullptr, *mdiag = nullptr, *rhs = nullptr;
-  double *pval = nullptr, *pdiag = nullptr, *pb = nullptr, *divStar = nullptr, *divCorr = nullptr;
-  double *phiStar = nullptr, *phi = nullptr;
-  double *bw[8] = {nullptr};  // BiCGSTAB work vectors (3*C each)
-  double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pq = nullptr, *pdx = nullptr;
-  double* pwdinv = nullptr;   // omega / pressure diagonal (level-0 smoother)
-  double* scal = nullptr;     // device scalars
-  int* flags = nullptr;
-  double* stats = nullptr;
-  double* forceOut = nullptr;
-  Reducer red{};
-  // pinned host mirrors
-  int* hFlags = nullptr;
-  double* hScal = nullptr;
-  double* hStage = nullptr;   // 3 * nCells staging for cell fields
-  // state
-  bool bcSet = false, stateSet = false, pZeroBC = true;
-  long long outerStep = 0;
-  int lastMomIts = 8, lastPIts = 8;
-  // AMG
-  bool amgBuilt = false;
-  AmgDev amg;
-  std::vector<AmgLevelHost> amgHost;
-  // measurement
-  Prof prof;
-  AlgoBytes ab;
-  // mixed precision (precision == ANB_PRECISION_MIXED): float matrices and inner-solver vectors
-  bool mixed = false;
-  float *mval32 = nullptr, *mdiag32 = nullptr, *pval32 = nullptr, *pdiag32 = nullptr, *pwdinv32 = nullptr;
-  float* bw32[8] = {nullptr};
-  float *r32 = nullptr, *dx32 = nullptr;                     // 3*nCells each
-  float *pr32 = nullptr, *pz32 = nullptr, *pp0_32 = nullptr, *pp1_32 = nullptr, *pq32 = nullptr;
-  AmgDevT<float> amg32;
-  double innerRtol = 1e-4;    // relative reduction asked of one FP32 inner solve at most
-  // scalar-library solves (allocated on first use)
-  DevArena scalarArena;
-  double *sMinv = nullptr, *sBcVal = nullptr, *sGamma = nullptr, *sFlux = nullptr, *sSrc = nullptr,
-         *sSp = nullptr, *sPhi = nullptr, *sGrad = nullptr;
-  uint8_t* sBcType = nullptr;
-};
-
-namespace {
 
 // Message of the last failed anb_create on this thread (anb_last_error(NULL)).
 thread_local std::string g_createError = "no context";
@@ -136,25 +22,6 @@ int fail(anb_ctx* c, const AnbError& e) {
   return e.code;
 }
 
-template <class F>
-int guarded(anb_ctx* c, F&& f) {
-  try {
-    return f();
-  } catch (const AnbError& e) {
-    return fail(c, e);
-  } catch (const std::bad_alloc&) {
-    if (c) c->err = "host allocation failed";
-    return ANB_ERR_INVALID;
-  } catch (const std::exception& e) {
-    if (c) c->err = e.what();
-    return ANB_ERR_MESH;
-  }
-}
-
-constexpr int kScalBicg = 0;    // 3 * 8
-constexpr int kScalPcg = 24;    // 8
-constexpr int kFlagBicg = 0;    // 3 * 4
-constexpr int kFlagPcg = 12;    // 4
 
 void permute_in(const anb_ctx* c, const double* src, std::vector<double>& dst, int comps) {
   dst.resize((size_t)comps * c->C);
@@ -793,7 +660,24 @@ void build_slot_lookup(anb_ctx* c) {
   }
 }
 
-}  // namespace
+void release_amg(anb_ctx* c) {
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
+  c->amg.graph = nullptr;
+  c->amg.graphKernels = 0;
+  c->amg.nLevels = 0;
+  c->amg.dense = nullptr;
+  if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
+  c->amg32.graph = nullptr;
+  c->amg32.graphKernels = 0;
+  c->amg32.nLevels = 0;
+  c->amg32.dense = nullptr;
+  c->amgArena.release();
+  c->amgHost.clear();
+  c->amgBuilt = false;
+}
+
+}  // namespace anb
 
 extern "C" {
 
@@ -1025,6 +909,7 @@ void anb_destroy(anb_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
   if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
+  adjoint_release(c);
   c->amgArena.release();
   c->arena.release();
   if (c->hFlags) cudaFreeHost(c->hFlags);
@@ -1169,23 +1054,6 @@ int anb_patch_force(anb_ctx* c, int patch, int sign, anb_force_report* out) {
 
 // ---- scalar libraries -------------------------------------------------------------------------
 namespace {
-
-void release_amg(anb_ctx* c) {
-  CK(cudaStreamSynchronize(c->stream));
-  if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
-  c->amg.graph = nullptr;
-  c->amg.graphKernels = 0;
-  c->amg.nLevels = 0;
-  c->amg.dense = nullptr;
-  if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
-  c->amg32.graph = nullptr;
-  c->amg32.graphKernels = 0;
-  c->amg32.nLevels = 0;
-  c->amg32.dense = nullptr;
-  c->amgArena.release();
-  c->amgHost.clear();
-  c->amgBuilt = false;
-}
 
 void ensure_scalar_buffers(anb_ctx* c) {
   if (c->sPhi) return;

@@ -306,4 +306,57 @@ void launch_defect(const LaunchCfg& lc, const DefectArgs& a);
 // x += dx (nc*n), dx = 0
 void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, float* dx);
 
+// ---- steady residual, tangent and adjoint (kernels_adjoint.cu) -----------------------------
+struct AdjArgs {
+  const double* U;    // 3*nCells converged velocity
+  const double* P;    // pressure
+  const double* G;    // 12*nCells: gradients of u, v, w, p (BC values from DMesh::bVal)
+  double* aP;         // unrelaxed momentum diagonal (written by adj_base)
+  double* rau;        // rAU of the SIMPLE iteration (written by adj_base)
+  double rho, mu, uRelax;
+  int relax;
+  Reducer red;
+};
+struct TanArgs {
+  const double* dU;   // 3*nCells
+  const double* dp;
+  const double* dg;   // 3*nBoundary tangent of the Dirichlet velocity values (0 off the parameters)
+  double dmu;
+  const double* dG;   // 12*nCells gradients of du, dv, dw (BC values dg) and dp (BC values 0)
+  double* daP;        // nCells work
+};
+struct AdjWork {
+  const double* w;    // 4*nCells adjoint weights (u | v | w | continuity)
+  double* abar;       // nCells work
+  double* h;          // 12*nCells work
+  double* gbar;       // 3*nBoundary adjoint of the Dirichlet velocity values, or null
+  double* muBar;      // 1 (device)
+};
+struct ObjArgs {
+  int b0, b1, sign;
+  double dir[3];
+  const double* bA;
+  const double* bN;
+  double* val;        // 2 (device): J, dJ/dmu at fixed (U, p)
+};
+void adj_base(const LaunchCfg& lc, const DMesh& m, const AdjArgs& a);
+void adj_residual(const LaunchCfg& lc, const DMesh& m, const AdjArgs& a, double* R);
+void adj_jvp(const LaunchCfg& lc, const DMesh& m, const AdjArgs& a, const TanArgs& t, double* dR);
+void adj_vjp(const LaunchCfg& lc, const DMesh& m, const AdjArgs& a, const AdjWork& w, double* out);
+void adj_objective(const LaunchCfg& lc, const DMesh& m, const AdjArgs& a, const ObjArgs& o, double* out);
+void adj_div_u(const LaunchCfg& lc, const DMesh& m, double rho, const double* v, double* y);
+void adj_div_u_t(const LaunchCfg& lc, const DMesh& m, double rho, const double* w, double* Y);
+// y = transpose of the LSQ gradient (field with Dirichlet bit dirBit) applied to fac*sc*s (s: 3C)
+void adj_grad_t(const LaunchCfg& lc, const DMesh& m, const double* sc, double fac, const double* s, double* h,
+                unsigned dirBit, double* y);
+// x (3C) -= fac * sc * gp
+void adj_sub_scaled_grad(const LaunchCfg& lc, int C, const double* sc, double fac, const double* gp, double* x);
+void adj_permute(const LaunchCfg& lc, int n, const int* idx, const double* src, double* dst);
+// out[j] = V_j . x for j < k (V: k vectors of length n, stride ld); partials: rowBlocks * k
+void vec_mdot(const LaunchCfg& lc, size_t n, int k, const double* V, size_t ld, const double* x, double* partials,
+              double* out);
+// x = beta x + sum_j coef[j] V_j (coef on the device)
+void vec_lincomb(const LaunchCfg& lc, size_t n, int k, const double* V, size_t ld, const double* coef, double beta,
+                 double* x);
+
 }  // namespace anb

@@ -185,6 +185,48 @@ int anb_scalar_transport_solve(anb_ctx* ctx, const double* face_flux, const doub
                                int nonorth_corr, double abs_tol, double rel_tol, int max_iter,
                                const double* x0, double* phi, anb_solve_info* info);
 
+/* ---- steady sensitivities (no counterpart in the reference) -----------------------------------
+ * At a converged SIMPLE state (U, p) the discrete steady residual R(U, p; g, mu) vanishes, with g
+ * the Dirichlet velocity values of the boundary faces and mu the viscosity.  For the objective
+ * J = dir . F, F the patch force of anb_patch_force, these entry points give dJ/dg and dJ/dmu
+ * (discrete adjoint) or dJ along one direction (tangent-linear).  Both solve one linear system
+ * with the exact Jacobian of R (hand-written tangent / transposed face-loop kernels) by FGMRES
+ * preconditioned with a SIMPLE-type block sweep (momentum BiCGSTAB on A or A^T, pressure AMG-PCG
+ * with the forward solver's hierarchy).  Nothing of the iteration history is stored: everything
+ * is recomputed from the converged state.  The state should be converged (see
+ * anb_steady_residual, anb_newton_solve); FP64 contexts only.  Boundary arrays have 3 x nFaces
+ * entries (u | v | w, input face order); only Dirichlet entries are meaningful. */
+typedef struct anb_adjoint_info {
+  int iterations;          /* FGMRES iterations (Newton: total over the steps) */
+  int converged;
+  double res_norm;         /* final residual two-norm of the linear system (Newton: of R) */
+  double rhs_norm;
+  double seconds;          /* wall time of the call */
+} anb_adjoint_info;
+
+/* Replaces the viscosity of the context (the next iteration and every sensitivity use it). */
+int anb_set_viscosity(anb_ctx* ctx, double mu);
+/* Steady residual R (4 x nCells: u | v | w | continuity, input cell order; may be NULL) and its
+ * two-norms (momentum, continuity) at the current state. */
+int anb_steady_residual(anb_ctx* ctx, double* res, double norms[2]);
+/* J = dir . F on the patch and its explicit mu-derivative at fixed (U, p). */
+int anb_force_objective(anb_ctx* ctx, int patch, int normal_sign, const double dir[3], double* J,
+                        double* dJ_dmu_explicit);
+/* Newton iterations on R = 0 from the current state (each an FGMRES solve to 1e-3 relative)
+ * until |R|_2 <= tol or max_newton steps; used to converge a perturbed state quickly. */
+int anb_newton_solve(anb_ctx* ctx, int max_newton, double tol, int lin_max_iter, int* steps,
+                     double* res_norm, anb_adjoint_info* info);
+/* dJ along (dbc, dmu): solves J_X dX = -R_theta dtheta (FGMRES to 1e-10 relative). */
+int anb_tangent_linear(anb_ctx* ctx, int patch, int normal_sign, const double dir[3], const double* dbc,
+                       double dmu, double* dJ, anb_adjoint_info* info);
+/* dJ/dg (3 x nFaces) and dJ/dmu: solves J_X^T lambda = dJ/dX (FGMRES to 1e-10 relative). */
+int anb_adjoint_force_grad(anb_ctx* ctx, int patch, int normal_sign, const double dir[3], double* dJ_dbc,
+                           double* dJ_dmu, double* J, anb_adjoint_info* info);
+/* Jacobian products for tests: dR = J dX + R_g dbc + R_mu dmu (dX 4 x nCells), and
+ * out = J^T w with gbc = R_g^T w, gmu = R_mu^T w. */
+int anb_debug_jvp(anb_ctx* ctx, const double* dX, const double* dbc, double dmu, double* dR);
+int anb_debug_vjp(anb_ctx* ctx, const double* w, double* out, double* gbc, double* gmu);
+
 /* ---- measurement (no counterpart in the reference; used by the benchmark) ------------------
  * Kernel families for anb_profile_select: every launch of the selected family is bracketed by
  * CUDA events on the context's stream and its algorithmic (compulsory) bytes are accumulated. */
