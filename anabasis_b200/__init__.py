@@ -62,7 +62,8 @@ class ForceReport(ct.Structure):
 
 class AdjointInfo(ct.Structure):
     _fields_ = [("iterations", ct.c_int), ("converged", ct.c_int), ("res_norm", ct.c_double),
-                ("rhs_norm", ct.c_double), ("seconds", ct.c_double)]
+                ("rhs_norm", ct.c_double), ("seconds", ct.c_double), ("prec_mom_its", ct.c_int),
+                ("prec_p_its", ct.c_int)]
 
 
 class SolveInfo(ct.Structure):
@@ -339,7 +340,7 @@ class Solver:
                                     ct.byref(info))
         self._check(rc, ok=(ANB_OK, ANB_NOT_CONVERGED))
         return dict(steps=steps.value, res_norm=rn.value, converged=rc == ANB_OK, iterations=info.iterations,
-                    seconds=info.seconds)
+                    seconds=info.seconds, prec_mom_its=info.prec_mom_its, prec_p_its=info.prec_p_its)
 
     def tangent_linear(self, patch, direction, dbc, dmu, normal_sign=-1) -> tuple[float, dict]:
         d = np.ascontiguousarray(direction, np.float64)

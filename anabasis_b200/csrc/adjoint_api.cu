@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 
 #include "context.hpp"
 
@@ -31,6 +32,16 @@ struct AdjointData {
   double* valT = nullptr;
   int* twin = nullptr;
   bool precReady = false;
+  // Preconditioner controls (ANB_ADJ_* environment variables override them).  The momentum
+  // block uses the SIMPLE iteration's own relaxed matrix (diagonal aP/uRelax): Jacobi-BiCGSTAB
+  // needs ~4 iterations on it against ~135 on the unrelaxed one, which made the adjoint 10x
+  // slower at 1M cells.  The pressure block is the pressure matrix scaled by rho/uRelax: for smooth
+  // pressure modes the Schur complement D_p - D_U A^-1 G is dominated by -D_U A^-1 G, which is
+  // the rAU/uRelax-weighted Laplacian, while the Rhie-Chow part D_p acts on the oscillatory ones.
+  int restart = 40;
+  double momRtol = 1e-2, pRtol = 1e-2, schur = 1.0;
+  int momMaxit = 200, momRelaxed = 1;
+  long long momIts = 0, pIts = 0;  // inner iterations since the last reset
 };
 
 void adjoint_release(anb_ctx* c) {
@@ -42,7 +53,12 @@ void adjoint_release(anb_ctx* c) {
 
 namespace {
 
-constexpr int kRestart = 40;
+constexpr int kMaxRestart = 120;
+
+double env_or(const char* name, double dflt) {
+  const char* v = std::getenv(name);
+  return v ? std::atof(v) : dflt;
+}
 
 AdjointData& adj(anb_ctx* c) {
   if (c->adj) return *c->adj;
@@ -53,7 +69,13 @@ AdjointData& adj(anb_ctx* c) {
   d->C = C;
   d->nB = c->nB;
   d->N = (size_t)4 * C;
-  d->mBasis = kRestart;
+  d->restart = std::max(4, std::min(kMaxRestart, (int)env_or("ANB_ADJ_RESTART", d->restart)));
+  d->momRtol = env_or("ANB_ADJ_MOM_RTOL", d->momRtol);
+  d->pRtol = env_or("ANB_ADJ_P_RTOL", d->pRtol);
+  d->schur = env_or("ANB_ADJ_SCHUR", c->prm.u_relax < 0.999999 ? c->prm.u_relax : 1.0);
+  d->momMaxit = (int)env_or("ANB_ADJ_MOM_MAXIT", d->momMaxit);
+  d->momRelaxed = (int)env_or("ANB_ADJ_MOM_RELAXED", d->momRelaxed);
+  d->mBasis = d->restart;
   d->aP = A.alloc<double>(C);
   d->rau = A.alloc<double>(C);
   d->G = A.alloc<double>((size_t)12 * C);
@@ -67,8 +89,8 @@ AdjointData& adj(anb_ctx* c) {
   d->zeroB = A.alloc<double>(c->nB);
   d->muBar = A.alloc<double>(2);
   d->objVal = A.alloc<double>(2);
-  d->partials = A.alloc<double>((size_t)c->lc.rowBlocks * (kRestart + 2));
-  d->coef = A.alloc<double>(kRestart + 2);
+  d->partials = A.alloc<double>((size_t)c->lc.rowBlocks * (d->mBasis + 2));
+  d->coef = A.alloc<double>(d->mBasis + 2);
   d->gX = A.alloc<double>(d->N);
   d->R = A.alloc<double>(d->N);
   d->t1 = A.alloc<double>(d->N);
@@ -76,8 +98,8 @@ AdjointData& adj(anb_ctx* c) {
   d->t3 = A.alloc<double>(d->N);
   d->xs = A.alloc<double>(d->N);
   d->rhs = A.alloc<double>(d->N);
-  d->V = A.alloc<double>((size_t)(kRestart + 1) * d->N);
-  d->Z = A.alloc<double>((size_t)kRestart * d->N);
+  d->V = A.alloc<double>((size_t)(d->mBasis + 1) * d->N);
+  d->Z = A.alloc<double>((size_t)d->mBasis * d->N);
   d->valT = A.alloc<double>(c->nEnt);
   CK(cudaMemsetAsync(d->dgZero, 0, sizeof(double) * 3 * c->nB, c->stream));
   CK(cudaMemsetAsync(d->zeroB, 0, sizeof(double) * c->nB, c->stream));
@@ -152,8 +174,9 @@ void vjp(anb_ctx* c, AdjointData& d, const double* w, double* out) {
 }
 
 // ---- preconditioner ---------------------------------------------------------------------------
-// Momentum matrix (unrelaxed, at the converged state), its transpose, the pressure matrix from
-// the same rAU the SIMPLE iteration uses, and its AMG hierarchy.
+// Momentum matrix at the converged state (relaxed as in the SIMPLE iteration, see AdjointData),
+// its transpose, the pressure matrix from the same rAU the SIMPLE iteration uses, and its AMG
+// hierarchy.
 void prec_setup(anb_ctx* c, AdjointData& d) {
   MomArgs ma{};
   ma.U = c->U;
@@ -161,8 +184,8 @@ void prec_setup(anb_ctx* c, AdjointData& d) {
   ma.G = d.G;
   ma.rho = c->prm.rho;
   ma.mu = c->prm.mu;
-  ma.uRelax = 1.0;
-  ma.relax = 0;
+  ma.uRelax = d.momRelaxed ? c->prm.u_relax : 1.0;
+  ma.relax = d.momRelaxed && c->prm.u_relax < 0.999999 ? 1 : 0;
   ma.rhsOnly = 0;
   ma.val = c->mval;
   ma.diag = c->mdiag;
@@ -190,7 +213,6 @@ void prec_setup(anb_ctx* c, AdjointData& d) {
   d.precReady = true;
 }
 
-constexpr double kPrecRtol = 1e-2;  // inner solves of the preconditioner (FGMRES tolerates them)
 
 // x (3C) = M^{-1} b with M the momentum matrix (transpose when trans), from x = 0
 void mom_solve(anb_ctx* c, AdjointData& d, bool trans, const double* b, double* x) {
@@ -204,8 +226,8 @@ void mom_solve(anb_ctx* c, AdjointData& d, bool trans, const double* b, double* 
   a.sc = c->scal + kScalBicg;
   a.fl = c->flags + kFlagBicg;
   a.atol = 0.0;
-  a.rtol = kPrecRtol;
-  a.maxit = 200;
+  a.rtol = d.momRtol;
+  a.maxit = d.momMaxit;
   a.red = c->red;
   CK(cudaMemsetAsync(x, 0, sizeof(double) * 3 * c->C, c->stream));
   bicg_init(c->lc, a);
@@ -216,11 +238,12 @@ void mom_solve(anb_ctx* c, AdjointData& d, bool trans, const double* b, double* 
     poll(c, a.fl, 12);
     if ((c->hFlags[0] && c->hFlags[4] && c->hFlags[8]) || done > a.maxit) break;
   }
+  d.momIts += std::max(c->hFlags[2], std::max(c->hFlags[6], c->hFlags[10]));
 }
 
-// x (C) = A_p^{-1} b / rho, from x = 0
-void p_solve(anb_ctx* c, const double* b, double* x) {
-  PcgArgs a = pcg_args(c, b, x, kPrecRtol);
+// x (C) = A_p^{-1} b, from x = 0 (the caller scales b)
+void p_solve(anb_ctx* c, AdjointData& d, const double* b, double* x) {
+  PcgArgs a = pcg_args(c, b, x, d.pRtol);
   a.atol = 0.0;
   a.maxit = 500;
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
@@ -234,6 +257,7 @@ void p_solve(anb_ctx* c, const double* b, double* x) {
     poll(c, a.fl, 4);
     if (c->hFlags[0] || it > a.maxit) break;
   }
+  d.pIts += c->hFlags[1];
 }
 
 void scale(anb_ctx* c, AdjointData& d, size_t n, const double* src, double s, double* dst) {
@@ -256,8 +280,8 @@ void precondition(anb_ctx* c, AdjointData& d, bool trans, const double* s, doubl
     mom_solve(c, d, false, s, zU);                                  // dU* = A^-1 s_U
     adj_div_u(c->lc, c->dm, rho, zU, d.t1);                         // D_U dU*
     CK(cudaMemcpyAsync(d.t2, s + 3 * (size_t)C, sizeof(double) * C, cudaMemcpyDeviceToDevice, c->stream));
-    axpby(c, d, C, -1.0 / rho, d.t1, 1.0 / rho, d.t2);              // (s_c - D_U dU*) / rho
-    p_solve(c, d.t2, zp);                                           // dp
+    axpby(c, d, C, -d.schur / rho, d.t1, d.schur / rho, d.t2);    // uRelax (s_c - D_U dU*) / rho
+    p_solve(c, d, d.t2, zp);                                        // dp
     GradArgs ga{};
     ga.nf = 1;
     ga.phi[0] = zp;
@@ -269,8 +293,8 @@ void precondition(anb_ctx* c, AdjointData& d, bool trans, const double* s, doubl
   } else {
     adj_grad_t(c->lc, c->dm, d.rau, fac, s, d.t3, 8u, d.t1);        // (Dinv G)^T s_U
     CK(cudaMemcpyAsync(d.t2, s + 3 * (size_t)C, sizeof(double) * C, cudaMemcpyDeviceToDevice, c->stream));
-    axpby(c, d, C, -1.0 / rho, d.t1, 1.0 / rho, d.t2);              // (s_c - ...) / rho
-    p_solve(c, d.t2, zp);
+    axpby(c, d, C, -d.schur / rho, d.t1, d.schur / rho, d.t2);    // uRelax (s_c - ...) / rho
+    p_solve(c, d, d.t2, zp);
     adj_div_u_t(c->lc, c->dm, rho, zp, d.t1);                       // D_U^T z_p
     CK(cudaMemcpyAsync(d.t2, s, sizeof(double) * 3 * C, cudaMemcpyDeviceToDevice, c->stream));
     axpby(c, d, 3 * (size_t)C, -1.0, d.t1, 1.0, d.t2);              // s_U - D_U^T z_p
@@ -408,8 +432,12 @@ ObjArgs obj_args(anb_ctx* c, AdjointData& d, int patch, int sign, const double d
   return o;
 }
 
-void fill_info(anb_adjoint_info* info, const KrylovResult& kr, double secs) {
+void fill_info(anb_adjoint_info* info, const KrylovResult& kr, double secs, const AdjointData* d = nullptr) {
   if (!info) return;
+  if (d) {
+    info->prec_mom_its = (int)d->momIts;
+    info->prec_p_its = (int)d->pIts;
+  }
   info->iterations = kr.its;
   info->converged = kr.conv ? 1 : 0;
   info->res_norm = kr.res;
@@ -545,6 +573,7 @@ int anb_newton_solve(anb_ctx* c, int maxNewton, double tol, int linMaxIt, int* s
     require(c);
     const auto t0 = std::chrono::steady_clock::now();
     AdjointData& d = adj(c);
+    d.momIts = d.pIts = 0;
     KrylovResult kr{};
     int k = 0, total = 0;
     double rn = 0.0;
@@ -565,7 +594,7 @@ int anb_newton_solve(anb_ctx* c, int maxNewton, double tol, int linMaxIt, int* s
     if (resNorm) *resNorm = rn;
     kr.its = total;
     kr.res = rn;
-    fill_info(info, kr, seconds_since(t0));
+    fill_info(info, kr, seconds_since(t0), &d);
     if (info) info->converged = rn <= tol ? 1 : 0;
     return rn <= tol ? ANB_OK : ANB_NOT_CONVERGED;
   });
@@ -578,6 +607,7 @@ int anb_tangent_linear(anb_ctx* c, int patch, int sign, const double dir[3], con
     require(c);
     const auto t0 = std::chrono::steady_clock::now();
     AdjointData& d = adj(c);
+    d.momIts = d.pIts = 0;
     base(c, d);
     prec_setup(c, d);
     upload_bc3(c, dbc, d.dgDir);
@@ -592,7 +622,7 @@ int anb_tangent_linear(anb_ctx* c, int patch, int sign, const double dir[3], con
     CK(cudaMemcpyAsync(v, d.objVal, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     *dJ = jx + v[1] * dmu;
-    fill_info(info, kr, seconds_since(t0));
+    fill_info(info, kr, seconds_since(t0), &d);
     return kr.conv ? ANB_OK : ANB_NOT_CONVERGED;
   });
 }
@@ -604,6 +634,7 @@ int anb_adjoint_force_grad(anb_ctx* c, int patch, int sign, const double dir[3],
     require(c);
     const auto t0 = std::chrono::steady_clock::now();
     AdjointData& d = adj(c);
+    d.momIts = d.pIts = 0;
     base(c, d);
     prec_setup(c, d);
     adj_objective(c->lc, c->dm, adj_args(c, d), obj_args(c, d, patch, sign, dir), d.gX);
@@ -620,7 +651,7 @@ int anb_adjoint_force_grad(anb_ctx* c, int patch, int sign, const double dir[3],
       const size_t n = (size_t)3 * (c->nI + c->nB);
       for (size_t i = 0; i < n; ++i) dJ_dbc[i] = -dJ_dbc[i];
     }
-    fill_info(info, kr, seconds_since(t0));
+    fill_info(info, kr, seconds_since(t0), &d);
     return kr.conv ? ANB_OK : ANB_NOT_CONVERGED;
   });
 }

@@ -292,6 +292,177 @@ def run_reference(args, rank: int) -> dict | None:
     }
 
 
+def _peak_device_bytes(device: int = 0) -> int | None:
+    """Device memory in use (NVML, read-only query).  The library allocates every buffer of a
+    phase up front and keeps it until the context is destroyed, so the figure taken at the end of
+    a phase is that phase's high-water mark."""
+    try:
+        import pynvml
+
+        pynvml.nvmlInit()
+        return int(pynvml.nvmlDeviceGetMemoryInfo(pynvml.nvmlDeviceGetHandleByIndex(device)).used)
+    except Exception:
+        return None
+
+
+def _converge(m, bc, precision, max_steps, tol_mass, tol_vel, init=None):
+    """SIMPLE from the initial state until massRes < tol_mass and max du < tol_vel."""
+    import anabasis_b200 as anb
+    from tests.cases import initial_state
+
+    s = anb.Solver(m, anb.default_params(precision=precision, **PARAMS))
+    s.set_bc(bc)
+    s.set_state(*(init if init is not None else initial_state(m, bc)))
+    _, st = s.iterate(max_steps, tol_mass, tol_vel)
+    names = m.topology()["patch_names"]
+    f = s.patch_force(names.index("patch_3_0"), -1)
+    return s, st, f
+
+
+def _field_errors(a: dict, b: dict) -> dict:
+    us = max(float(np.abs(a[k]).max()) for k in "uvw")
+    e = {k: float(np.abs(a[k] - b[k]).max()) / us for k in "uvw"}
+    e["p"] = float(np.abs(a["p"] - b["p"]).max()) / max(float(np.abs(a["p"]).max()), 1e-300)
+    return e
+
+
+def run_mixed4m(args) -> dict:
+    """Config 3: 320x112x112 jittered obstacle channel (seed 1), FP64 and mixed precision each run
+    from the initial state to massRes < 1e-6 and max relative velocity change < tol_vel; time
+    ratio, field and force errors of the mixed run against the FP64 run."""
+    from tests.cases import channel
+
+    m, bc, _ = channel(nx=320, ny=112, nz=112, jitter=0.15, seed=1, obstacle=True)
+    runs = {}
+    for prec in (0, 1):
+        t0 = time.perf_counter()
+        s, st, f = _converge(m, bc, prec, args.max_steps, 1e-6, args.tol_vel)
+        wall = time.perf_counter() - t0
+        runs[prec] = dict(steps=len(st), device_s=float(sum(x["iter_seconds"] for x in st)), wall_s=wall,
+                          mass_res=st[-1]["mass_res"], du=max(st[-1]["du_rel"], st[-1]["dv_rel"], st[-1]["dw_rel"]),
+                          F=f["F"], state=s.get_state(with_phi=False), peak_bytes=_peak_device_bytes())
+        s.close()
+    a, b = runs[0], runs[1]
+    F = np.array(a["F"])
+    ferr = float(np.abs(np.array(b["F"]) - F).max() / np.abs(F).max())
+    strip = lambda r: {k: v for k, v in r.items() if k != "state"}  # noqa: E731
+    return {"metric": "time to converged solution (massRes<1e-6), FP64 / mixed precision", "value": a["device_s"] / b["device_s"],
+            "unit": "x", "higher_is_better": True, "n_gpus": 1, "dtype": "f64 vs f32-inner/f64-outer",
+            "data": "synthetic",
+            "config": {"workload": "obstacle channel 320x112x112 jittered hex (seed 1), 2 non-orthogonal correctors",
+                       "cells": m.n_cells, "tol_mass": 1e-6, "tol_vel": args.tol_vel},
+            "fp64": strip(a), "mixed": strip(b), "force_rel_error": ferr, "field_rel_error": _field_errors(a["state"], b["state"])}
+
+
+def run_adjoint1m(args) -> dict:
+    """Config 4: 1M-cell obstacle channel; converged FP64 forward (SIMPLE, then Newton to a residual
+    two-norm of 1e-13), adjoint gradient of the x-force on the obstacle w.r.t. every inlet-face
+    velocity and mu, checked against the tangent-linear model and central differences (h = 1e-6
+    along unit random directions, seed 42, each perturbed state Newton-converged)."""
+    from tests.cases import channel
+
+    m, bc, _ = channel(**WORKLOAD)
+    t0 = time.perf_counter()
+    s, st, _ = _converge(m, bc, 0, args.max_steps, 1e-10, 1e-8)
+    fwd_dev = float(sum(x["iter_seconds"] for x in st))
+    fwd_wall = time.perf_counter() - t0
+    newton = s.newton_solve(max_newton=10, tol=1e-13)
+    names = m.topology()["patch_names"]
+    k_in, k_obs = names.index("patch_1_0"), names.index("patch_3_0")
+    direction = (1.0, 0.0, 0.0)
+    g, gmu, J, ainfo = s.adjoint_force_grad(k_obs, direction)
+    t = m.topology()
+    F = m.n_faces
+    mask = np.zeros(F, bool)
+    s0, n = int(t["patch_start"][k_in]), int(t["patch_size"][k_in])
+    mask[s0:s0 + n] = True
+    mask = np.tile(mask, 3)
+    base = s.get_state(with_phi=False)
+    rng = np.random.default_rng(42)
+    checks = []
+    h = 1e-6
+    for i in range(args.dirs):
+        d = np.where(mask, rng.standard_normal(3 * F), 0.0)
+        dmu = rng.standard_normal()
+        nrm = np.sqrt(d @ d + dmu * dmu)
+        d, dmu = d / nrm, dmu / nrm
+        adj = float(g @ d + gmu * dmu)
+        rec = {"adjoint": adj}
+        if i < args.tl_dirs:
+            tl, tinfo = s.tangent_linear(k_obs, direction, d, dmu)
+            rec.update(tangent_linear=tl, tl_rel_err=abs(tl - adj) / abs(adj), tl_seconds=tinfo["seconds"])
+        Jpm = []
+        for sg in (1.0, -1.0):
+            s.set_state(base["u"], base["v"], base["w"], base["p"])
+            b = dict(bc)
+            for q, k in enumerate("uvw"):
+                b[k] = bc[k] + sg * h * d[q * F:(q + 1) * F]
+            s.set_bc(b)
+            s.set_viscosity(PARAMS["mu"] + sg * h * dmu)
+            s.newton_solve(max_newton=10, tol=1e-13)
+            Jpm.append(s.force_objective(k_obs, direction)[0])
+        fd = (Jpm[0] - Jpm[1]) / (2 * h)
+        rec.update(fd=fd, fd_rel_err=abs(fd - adj) / abs(adj))
+        checks.append(rec)
+        s.set_state(base["u"], base["v"], base["w"], base["p"])
+        s.set_bc(bc)
+        s.set_viscosity(PARAMS["mu"])
+    return {"metric": "adjoint cost / forward cost", "value": ainfo["seconds"] / fwd_dev, "unit": "x",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "obstacle channel 200x70x70 jittered hex (970480 cells), J = x-force on the "
+                                   "obstacle, parameters 3 x inlet-face velocities + mu", "cells": m.n_cells,
+                       "inlet_faces": int(n), "fd_step": h, "directions": args.dirs},
+            "forward": {"simple_steps": len(st), "device_s": fwd_dev, "wall_s": fwd_wall, "newton": newton},
+            "adjoint": ainfo, "J": J, "dJ_dmu": gmu,
+            "max_fd_rel_err": max(c["fd_rel_err"] for c in checks) if checks else None,
+            "max_tl_rel_err": max((c["tl_rel_err"] for c in checks if "tl_rel_err" in c), default=None),
+            "checks": checks}
+
+
+def run_tets16m(args) -> dict:
+    """Config 5: 463x76x76 jittered hexes (seed 2) split into 6 tets, obstacle removed before the
+    split (~16M cells).  Mixed-precision forward for --steps SIMPLE steps from the initial state,
+    the same steps in FP64 as the accuracy judge, then the adjoint gradient of the obstacle force at
+    the FP64 state restored from a host checkpoint of (U, p) in a fresh FP64 context; peak device
+    memory of each phase."""
+    import anabasis_b200 as anb
+    from tests.cases import channel
+
+    t0 = time.perf_counter()
+    m, bc, _ = channel(nx=463, ny=76, nz=76, jitter=0.15, seed=2, obstacle=True, tets=True)
+    mesh_s = time.perf_counter() - t0
+    out = {"metric": "mixed-precision SIMPLE cell-iters/s at 16M tets", "unit": "cell-iters/s", "n_gpus": 1,
+           "higher_is_better": True, "data": "synthetic",
+           "config": {"workload": "463x76x76 jittered hexes split into 6 tets, obstacle channel", "cells": m.n_cells,
+                      "steps": args.steps}, "mesh_build_s": mesh_s}
+    runs = {}
+    for prec in (1, 0):
+        t0 = time.perf_counter()
+        s, st, f = _converge(m, bc, prec, args.steps, -1.0, -1.0)
+        runs[prec] = dict(device_s=float(sum(x["iter_seconds"] for x in st[1:])), steps=len(st), F=f["F"],
+                          setup_and_run_wall_s=time.perf_counter() - t0, peak_bytes=_peak_device_bytes(),
+                          state=s.get_state(with_phi=False))
+        s.close()
+    out["value"] = m.n_cells * (runs[1]["steps"] - 1) / runs[1]["device_s"]
+    out["fp64_cell_iters_per_s"] = m.n_cells * (runs[0]["steps"] - 1) / runs[0]["device_s"]
+    F = np.array(runs[0]["F"])
+    out["mixed_vs_fp64"] = {"force_rel_error": float(np.abs(np.array(runs[1]["F"]) - F).max() / np.abs(F).max()),
+                            "field_rel_error": _field_errors(runs[0]["state"], runs[1]["state"])}
+    ck = runs[0]["state"]
+    s = anb.Solver(m, anb.default_params(**PARAMS))
+    s.set_bc(bc)
+    s.set_state(ck["u"], ck["v"], ck["w"], ck["p"])
+    names = m.topology()["patch_names"]
+    _, res = s.steady_residual()
+    g, gmu, J, ainfo = s.adjoint_force_grad(names.index("patch_3_0"), (1.0, 0.0, 0.0))
+    out["adjoint"] = dict(ainfo, dJ_dmu=gmu, J=J, residual_norms=list(map(float, res)),
+                          peak_bytes=_peak_device_bytes())
+    for k in (0, 1):
+        runs[k].pop("state")
+    out["mixed"], out["fp64"] = runs[1], runs[0]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -299,14 +470,24 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--config", default="obstacle1m", choices=["obstacle1m", "mixed4m", "adjoint1m", "tets16m"],
+                    help="obstacle1m: the headline SIMPLE throughput line; the others are single-GPU studies "
+                         "of the mixed-precision, adjoint and 16M-tet configurations")
+    ap.add_argument("--max-steps", type=int, default=4000)
+    ap.add_argument("--tol-vel", type=float, default=1e-6)
+    ap.add_argument("--dirs", type=int, default=8, help="adjoint1m: finite-difference directions")
+    ap.add_argument("--tl-dirs", type=int, default=4, help="adjoint1m: tangent-linear directions")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    studies = {"mixed4m": run_mixed4m, "adjoint1m": run_adjoint1m, "tets16m": run_tets16m}
     if args.impl == "reference":
         out = run_reference(args, rank)
+    elif args.config in studies:
+        out = studies[args.config](args) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None:

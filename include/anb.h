@@ -202,6 +202,8 @@ typedef struct anb_adjoint_info {
   double res_norm;         /* final residual two-norm of the linear system (Newton: of R) */
   double rhs_norm;
   double seconds;          /* wall time of the call */
+  int prec_mom_its;        /* preconditioner work: momentum BiCGSTAB iterations (max component) */
+  int prec_p_its;          /* and pressure PCG iterations, summed over the applications */
 } anb_adjoint_info;
 
 /* Replaces the viscosity of the context (the next iteration and every sensitivity use it). */
