@@ -217,7 +217,7 @@ void prec_setup(anb_ctx* c, AdjointData& d) {
 // x (3C) = M^{-1} b with M the momentum matrix (transpose when trans), from x = 0
 void mom_solve(anb_ctx* c, AdjointData& d, bool trans, const double* b, double* x) {
   BicgArgs a{};
-  a.A = DSell{c->C, c->dm.sliceOff, c->dm.col, trans ? d.valT : c->mval, c->mdiag};
+  a.A = DSell{c->C, c->dm.sliceOff, c->dm.col, trans ? d.valT : c->mval, c->mdiag, c->L.maxRowLen};
   a.nc = 3;
   a.b = b;
   a.x = x;

@@ -84,8 +84,10 @@ void download_offdiag(anb_ctx* c, const double* val, double* a_pn, double* a_np)
   }
 }
 
-DSell mom_sell(const anb_ctx* c) { return DSell{c->C, c->L.sliceOff.empty() ? nullptr : c->dm.sliceOff, c->dm.col, c->mval, c->mdiag}; }
-DSell p_sell(const anb_ctx* c) { return DSell{c->C, c->dm.sliceOff, c->dm.col, c->pval, c->pdiag}; }
+DSell mom_sell(const anb_ctx* c) {
+  return DSell{c->C, c->L.sliceOff.empty() ? nullptr : c->dm.sliceOff, c->dm.col, c->mval, c->mdiag, c->L.maxRowLen};
+}
+DSell p_sell(const anb_ctx* c) { return DSell{c->C, c->dm.sliceOff, c->dm.col, c->pval, c->pdiag, c->L.maxRowLen}; }
 
 void grad(anb_ctx* c, int nf, const double* const* phi, const unsigned char* bits, double* const* out) {
   GradArgs a{};
@@ -213,7 +215,7 @@ void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* it
 
 PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, double rtol) {
   PcgArgsT<float> a{};
-  a.A = DSellT<float>{c->C, c->dm.sliceOff, c->dm.col, c->pval32, c->pdiag32};
+  a.A = DSellT<float>{c->C, c->dm.sliceOff, c->dm.col, c->pval32, c->pdiag32, c->L.maxRowLen};
   a.b = b;
   a.x = x;
   a.r = c->pr32; a.z = c->pz32; a.p0 = c->pp0_32; a.p1 = c->pp1_32; a.q = c->pq32;
@@ -251,6 +253,7 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
       d.val = val0;
       d.diag = diag0;
       d.wdinv = wdinv0;
+      d.maxW = c->L.maxRowLen;
     } else {
       d.rowOff = ar.upload(h.rowOff);
       d.col = ar.upload(h.col);
@@ -306,7 +309,7 @@ constexpr int kFlagFrozen = 28;  // 3
 void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
   const int C = c->C;
   DefectArgs d{};
-  d.A = DSellT<float>{C, c->dm.sliceOff, c->dm.col, c->mval32, c->mdiag32};
+  d.A = DSellT<float>{C, c->dm.sliceOff, c->dm.col, c->mval32, c->mdiag32, c->L.maxRowLen};
   d.nc = 3;
   d.b = c->rhs;
   d.x = c->Us;
@@ -383,7 +386,7 @@ void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3
 
 void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
   DefectArgs d{};
-  d.A = DSellT<float>{c->C, c->dm.sliceOff, c->dm.col, c->pval32, c->pdiag32};
+  d.A = DSellT<float>{c->C, c->dm.sliceOff, c->dm.col, c->pval32, c->pdiag32, c->L.maxRowLen};
   d.nc = 1;
   d.b = b;
   d.x = x;

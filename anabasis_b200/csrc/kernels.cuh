@@ -255,6 +255,7 @@ struct AmgLevelDevT {
   // work vectors
   T *b, *x, *x2;
   T* wdinv;            // omega / diag (Jacobi smoother)
+  int maxW;            // level 0: largest SELL slice width
 };
 template <class T>
 struct AmgDevT {

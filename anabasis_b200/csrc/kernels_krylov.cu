@@ -59,6 +59,56 @@ __device__ __forceinline__ void sell_row3(const DSellT<T>& A, int r, const T* x,
   }
 }
 
+// Row r's slots in registers, for a compile-time bound WM on the slice width: every column and
+// value load of the row is issued before the first gather, so a row costs two dependent memory
+// round trips instead of two per unrolled group.  Slots past the row's slice width are
+// (column r, value 0) and read nothing.
+template <int WM, class T>
+__device__ __forceinline__ void sell_regs(const int* sliceOff, const int* col, const T* val, int r, int (&c)[WM],
+                                          double (&v)[WM]) {
+  const int s = r >> 5;
+  const int b0 = __ldg(&sliceOff[s]);
+  const int W = (__ldg(&sliceOff[s + 1]) - b0) >> 5;
+  const int b = b0 + (r & 31);
+#pragma unroll
+  for (int k = 0; k < WM; ++k) {
+    c[k] = r;
+    v[k] = 0.0;
+    if (k < W) {
+      c[k] = __ldg(&col[b + (k << 5)]);
+      v[k] = ld(&val[b + (k << 5)]);
+    }
+  }
+}
+
+// sell_row3 with the row in registers
+template <int WM, class T>
+__device__ __forceinline__ void sell_row3_regs(const DSellT<T>& A, int r, const T* x, size_t n, const bool* act, int nc,
+                                               double* y) {
+  int c[WM];
+  double v[WM];
+  sell_regs<WM>(A.sliceOff, A.col, A.val, r, c, v);
+  const double d = (double)A.diag[r];
+  for (int q = 0; q < 3; ++q) {
+    if (!(q < nc && act[q])) {
+      y[q] = 0.0;
+      continue;
+    }
+    const T* xq = x + q * n;
+    double acc = d * (double)xq[r];
+#pragma unroll
+    for (int k = 0; k < WM; ++k) acc += v[k] * (double)xq[c[k]];
+    y[q] = acc;
+  }
+}
+
+template <int WM, class T>
+__device__ __forceinline__ void row3(const DSellT<T>& A, int r, const T* x, size_t n, const bool* act, int nc,
+                                     double* y) {
+  if constexpr (WM == 0) sell_row3(A, r, x, n, act, nc, y);
+  else sell_row3_regs<WM>(A, r, x, n, act, nc, y);
+}
+
 // ---------------------------------------------------------------- BiCGSTAB, nc components
 // scalars per component c: sc[8c + 0..7] = rho, rhoN, alpha, omega, eps, rn, -, -
 // flags per component c:   fl[4c + 0..3] = done, half, iters, converged
@@ -132,7 +182,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgsT<T> a) {
 }
 
 // v = A ph ; alpha = rhoN / (rh . v) ; rho = rhoN
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgsT<T> a) {
   __shared__ double sm[3 * 32];
   if (all_done(a.fl, a.nc)) return;
@@ -142,7 +192,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgsT<T> a) {
   double acc[3] = {0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     double y[3];
-    sell_row3(a.A, r, a.ph, (size_t)n, act, a.nc, y);
+    row3<WM>(a.A, r, a.ph, (size_t)n, act, a.nc, y);
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
@@ -197,7 +247,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgsT<T> a) {
 }
 
 // t = A sh ; omega = (t.s)/(t.t)
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgsT<T> a) {
   __shared__ double sm[6 * 32];
   if (all_done(a.fl, a.nc)) return;
@@ -207,7 +257,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgsT<T> a) {
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     double y[3];
-    sell_row3(a.A, r, a.sh, (size_t)n, act, a.nc, y);
+    row3<WM>(a.A, r, a.sh, (size_t)n, act, a.nc, y);
     for (int c = 0; c < a.nc; ++c) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
@@ -325,7 +375,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_jacobi(PcgArgsT<T> a) {
 }
 
 // pNew = z + beta pOld (rows and, on the fly, their neighbours); q = A pNew; alpha = rz / (p.q)
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld, T* pNew) {
   __shared__ double sm[32];
   if (a.fl[0]) return;
@@ -333,15 +383,23 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld,
   const double beta = a.fl[3] ? 0.0 : a.sc[2];
   double acc[1] = {0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const int s = r >> 5;
-    const int b = __ldg(&a.A.sliceOff[s]) + (r & 31);
-    const int W = (__ldg(&a.A.sliceOff[s + 1]) - __ldg(&a.A.sliceOff[s])) >> 5;
     const double pr = (double)(T)((double)a.z[r] + beta * (double)pOld[r]);
     double q = (double)a.A.diag[r] * pr;
-    for (int k = 0; k < W; ++k) {
-      const int e = b + (k << 5);
-      const int c = __ldg(&a.A.col[e]);
-      q += (double)a.A.val[e] * (double)(T)((double)a.z[c] + beta * (double)pOld[c]);
+    if constexpr (WM == 0) {
+      const int s = r >> 5;
+      const int b = __ldg(&a.A.sliceOff[s]) + (r & 31);
+      const int W = (__ldg(&a.A.sliceOff[s + 1]) - __ldg(&a.A.sliceOff[s])) >> 5;
+      for (int k = 0; k < W; ++k) {
+        const int e = b + (k << 5);
+        const int c = __ldg(&a.A.col[e]);
+        q += (double)a.A.val[e] * (double)(T)((double)a.z[c] + beta * (double)pOld[c]);
+      }
+    } else {
+      int c[WM];
+      double v[WM];
+      sell_regs<WM>(a.A.sliceOff, a.A.col, a.A.val, r, c, v);
+#pragma unroll
+      for (int k = 0; k < WM; ++k) q += v[k] * (double)(T)((double)a.z[c[k]] + beta * (double)pOld[c[k]]);
     }
     pNew[r] = (T)pr;
     a.q[r] = (T)q;
@@ -385,7 +443,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgsT<T> a, const T* p) {
 // Down, part 1: weighted-Jacobi pre-smoothing from zero (x = w D^-1 b) fused with the residual
 // r = b - A x (neighbour x computed on the fly); thread per row, SELL-coalesced.  r goes to x2,
 // which is free until the up sweep.
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelDevT<T> f, double omega) {
   if (*done) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
@@ -393,14 +451,22 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
     const double bi = ld(&f.b[i]);
     const double xi = ld(&f.wdinv[i]) * bi;
     double ax = di * xi;
-    const int s = i >> 5;
-    const int b = __ldg(&f.sliceOff[s]) + (i & 31);
-    const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
+    if constexpr (WM == 0) {
+      const int s = i >> 5;
+      const int b = __ldg(&f.sliceOff[s]) + (i & 31);
+      const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
 #pragma unroll 4
-    for (int k = 0; k < W; ++k) {
-      const int e = b + (k << 5);
-      const int j = __ldg(&f.col[e]);
-      ax += ld(&f.val[e]) * (ld(&f.wdinv[j]) * ld(&f.b[j]));
+      for (int k = 0; k < W; ++k) {
+        const int e = b + (k << 5);
+        const int j = __ldg(&f.col[e]);
+        ax += ld(&f.val[e]) * (ld(&f.wdinv[j]) * ld(&f.b[j]));
+      }
+    } else {
+      int c[WM];
+      double v[WM];
+      sell_regs<WM>(f.sliceOff, f.col, f.val, i, c, v);
+#pragma unroll
+      for (int k = 0; k < WM; ++k) ax += v[k] * (ld(&f.wdinv[c[k]]) * ld(&f.b[c[k]]));
     }
     f.x[i] = (T)xi;
     f.x2[i] = (T)(bi - ax);
@@ -488,7 +554,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLev
 // Up: prolongate the coarse correction and post-smooth (one weighted-Jacobi sweep) in one pass:
 // xt_j = x_j + corr * e[agg(j)] on the fly, out_i = xt_i + w D^-1 (b_i - (A xt)_i).
 // On level 0 it also forms r.z for the PCG recurrence.
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevelDevT<T> f, const T* e, double omega,
                                                    double corr, T* out, int finest, PcgArgsT<T> a) {
   __shared__ double sm[32];
@@ -498,15 +564,26 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
     const double di = ld(&f.diag[i]);
     const double xi = ld(&f.x[i]) + corr * ld(&e[__ldg(&f.agg[i])]);
     double ax = di * xi;
-    const int s = i >> 5;
-    const int b = __ldg(&f.sliceOff[s]) + (i & 31);
-    const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
-    // unrolled so the col -> agg -> e load chains of several entries are in flight together
+    if constexpr (WM == 0) {
+      const int s = i >> 5;
+      const int b = __ldg(&f.sliceOff[s]) + (i & 31);
+      const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
+      // unrolled so the col -> agg -> e load chains of several entries are in flight together
 #pragma unroll 4
-    for (int k = 0; k < W; ++k) {
-      const int ee = b + (k << 5);
-      const int j = __ldg(&f.col[ee]);
-      ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
+      for (int k = 0; k < W; ++k) {
+        const int ee = b + (k << 5);
+        const int j = __ldg(&f.col[ee]);
+        ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
+      }
+    } else {
+      int c[WM];
+      double v[WM];
+      sell_regs<WM>(f.sliceOff, f.col, f.val, i, c, v);
+      int g[WM];
+#pragma unroll
+      for (int k = 0; k < WM; ++k) g[k] = __ldg(&f.agg[c[k]]);
+#pragma unroll
+      for (int k = 0; k < WM; ++k) ax += v[k] * (ld(&f.x[c[k]]) + corr * ld(&e[g[k]]));
     }
     const double bi = (double)f.b[i];
     const T xn = (T)(xi + ld(&f.wdinv[i]) * (bi - ax));
@@ -665,9 +742,12 @@ void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
     ProfScope ps(lc, kKfBicgVector, 0.0);
     k_bicg_p<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
+  const int wc = sell_width_class(a.A.maxW);
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
-    k_bicg_v<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    if (wc == 4) k_bicg_v<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    else if (wc == 8) k_bicg_v<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    else k_bicg_v<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
@@ -675,7 +755,9 @@ void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
   }
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
-    k_bicg_t<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    if (wc == 4) k_bicg_t<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    else if (wc == 8) k_bicg_t<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    else k_bicg_t<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
@@ -700,7 +782,11 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
   {
     const AmgLevelDevT<T>& f = amg->lv[0];
     ProfScope ps(lc, kKfAmgResid0, 0.0, 2);
-    k_amg_resid<T><<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+    const int wc = sell_width_class(f.maxW);
+    const int nb = blocks_for(f.n, lc.rowBlocks);
+    if (wc == 4) k_amg_resid<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+    else if (wc == 8) k_amg_resid<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+    else k_amg_resid<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
@@ -725,8 +811,11 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     const AmgLevelDevT<T>& f = amg->lv[0];
     const T* e = (L == 2) ? amg->lv[1].x : amg->lv[1].x2;
     ProfScope ps(lc, kKfAmgUp0, 0.0);
-    k_amg_up<T><<<blocks_for(f.n, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1,
-                                                                          a);
+    const int wc = sell_width_class(f.maxW);
+    const int nb = blocks_for(f.n, lc.rowBlocks);
+    if (wc == 4) k_amg_up<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
+    else if (wc == 8) k_amg_up<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
+    else k_amg_up<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
   }
 }
 
@@ -777,7 +866,10 @@ void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgD
     // values and vectors halve in FP32
     const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
     ProfScope ps(lc, kKfPcgSpmv, by);
-    k_pcg_pq<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+    const int wc = sell_width_class(a.A.maxW);
+    if (wc == 4) k_pcg_pq<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+    else if (wc == 8) k_pcg_pq<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+    else k_pcg_pq<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
   }
   {
     ProfScope ps(lc, kKfPcgUpdate, 0.0);
