@@ -25,6 +25,8 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 HOST_SOURCES = ["host_mesh.cpp", "host_case.cpp", "host_output.cpp", "host_api.cpp", "layout.cpp", "amg_setup.cpp"]
+MMS_APPS = {1: "anabasis_poisson_mms", 2: "anabasis_poisson_mms_neumann", 3: "anabasis_poisson_mms_mixed",
+            4: "anabasis_scalar_mms"}
 CUDA_SOURCES = ["kernels_fv.cu", "kernels_krylov.cu", "kernels_scalar.cu", "kernels_adjoint.cu", "anb_api.cu", "adjoint_api.cu", "nalloc.cu"]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
 NVCCFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr"]
@@ -81,6 +83,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or _stale(app, [app_obj, lib]):
         _run(["g++", "-o", str(app), str(app_obj), f"-L{LIB}", "-lanb", f"-L{CUDA_HOME}/lib64", "-lcudart",
               "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{CUDA_HOME}/lib64", "-fopenmp"])
+    # the reference's manufactured-solution programs, one executable each from app_mms.cpp
+    mms_src = CSRC / "app_mms.cpp"
+    for idx, name in MMS_APPS.items():
+        exe = LIB / name
+        if force or _stale(exe, [mms_src, lib] + hdrs):
+            _run(["g++", *CXXFLAGS, f"-DANB_MMS_APP={idx}", f"-I{CUDA_HOME}/include", "-o", str(exe), str(mms_src),
+                  f"-L{LIB}", "-lanb", f"-L{CUDA_HOME}/lib64", "-lcudart", "-Wl,-rpath,$ORIGIN",
+                  f"-Wl,-rpath,{CUDA_HOME}/lib64"])
     return lib
 
 

@@ -39,6 +39,7 @@ struct AdjointData {
   // pressure modes the Schur complement D_p - D_U A^-1 G is dominated by -D_U A^-1 G, which is
   // the rAU/uRelax-weighted Laplacian, while the Rhie-Chow part D_p acts on the oscillatory ones.
   int restart = 40;
+  double rtol = 1e-10;  // relative tolerance of the tangent-linear and adjoint systems
   double momRtol = 1e-2, pRtol = 1e-2, schur = 1.0;
   int momMaxit = 200, momRelaxed = 1;
   long long momIts = 0, pIts = 0;  // inner iterations since the last reset
@@ -70,6 +71,7 @@ AdjointData& adj(anb_ctx* c) {
   d->nB = c->nB;
   d->N = (size_t)4 * C;
   d->restart = std::max(4, std::min(kMaxRestart, (int)env_or("ANB_ADJ_RESTART", d->restart)));
+  d->rtol = env_or("ANB_ADJ_RTOL", d->rtol);
   d->momRtol = env_or("ANB_ADJ_MOM_RTOL", d->momRtol);
   d->pRtol = env_or("ANB_ADJ_P_RTOL", d->pRtol);
   d->schur = env_or("ANB_ADJ_SCHUR", c->prm.u_relax < 0.999999 ? c->prm.u_relax : 1.0);
@@ -614,7 +616,7 @@ int anb_tangent_linear(anb_ctx* c, int patch, int sign, const double dir[3], con
     CK(cudaMemsetAsync(d.t1, 0, sizeof(double) * d.N, c->stream));
     jvp(c, d, d.t1, d.dgDir, dmu, d.rhs);  // R_theta dtheta
     scale(c, d, d.N, d.rhs, -1.0, d.rhs);
-    KrylovResult kr = fgmres(c, d, false, d.rhs, d.xs, 1e-10, 2000);
+    KrylovResult kr = fgmres(c, d, false, d.rhs, d.xs, d.rtol, 2000);
     adj_objective(c->lc, c->dm, adj_args(c, d), obj_args(c, d, patch, sign, dir), d.gX);
     vec_mdot(c->lc, d.N, 1, d.gX, d.N, d.xs, d.partials, d.coef);
     double v[2], jx = 0.0;
@@ -638,7 +640,7 @@ int anb_adjoint_force_grad(anb_ctx* c, int patch, int sign, const double dir[3],
     base(c, d);
     prec_setup(c, d);
     adj_objective(c->lc, c->dm, adj_args(c, d), obj_args(c, d, patch, sign, dir), d.gX);
-    KrylovResult kr = fgmres(c, d, true, d.gX, d.xs, 1e-10, 2000);  // J^T lambda = dJ/dX
+    KrylovResult kr = fgmres(c, d, true, d.gX, d.xs, d.rtol, 2000);  // J^T lambda = dJ/dX
     vjp(c, d, d.xs, d.t1);                                           // gbar = R_g^T lambda, muBar
     double v[2], mb = 0.0;
     CK(cudaMemcpyAsync(v, d.objVal, sizeof(v), cudaMemcpyDeviceToHost, c->stream));

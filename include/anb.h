@@ -218,10 +218,11 @@ int anb_force_objective(anb_ctx* ctx, int patch, int normal_sign, const double d
  * until |R|_2 <= tol or max_newton steps; used to converge a perturbed state quickly. */
 int anb_newton_solve(anb_ctx* ctx, int max_newton, double tol, int lin_max_iter, int* steps,
                      double* res_norm, anb_adjoint_info* info);
-/* dJ along (dbc, dmu): solves J_X dX = -R_theta dtheta (FGMRES to 1e-10 relative). */
+/* dJ along (dbc, dmu): solves J_X dX = -R_theta dtheta (FGMRES to 1e-10 relative; the environment
+ * variable ANB_ADJ_RTOL, read when a context first uses these entry points, changes it). */
 int anb_tangent_linear(anb_ctx* ctx, int patch, int normal_sign, const double dir[3], const double* dbc,
                        double dmu, double* dJ, anb_adjoint_info* info);
-/* dJ/dg (3 x nFaces) and dJ/dmu: solves J_X^T lambda = dJ/dX (FGMRES to 1e-10 relative). */
+/* dJ/dg (3 x nFaces) and dJ/dmu: solves J_X^T lambda = dJ/dX (FGMRES, same tolerance). */
 int anb_adjoint_force_grad(anb_ctx* ctx, int patch, int normal_sign, const double dir[3], double* dJ_dbc,
                            double* dJ_dmu, double* J, anb_adjoint_info* info);
 /* Jacobian products for tests: dR = J dX + R_g dbc + R_mu dmu (dX 4 x nCells), and
