@@ -1017,7 +1017,8 @@ int anb_simple_iterate(anb_ctx* c, int nsteps, double tolMass, double tolVel, an
       if (simple_step(c, &st) == ANB_NOT_CONVERGED) status = ANB_NOT_CONVERGED;
       if (stats) stats[k] = st;
       if (done) *done = k + 1;
-      if (!std::isfinite(st.mass_res) || st.mass_res > 1e50) {
+      if (!std::isfinite(st.mass_res) || st.mass_res > 1e50 || !std::isfinite(st.du_rel) ||
+          !std::isfinite(st.dv_rel) || !std::isfinite(st.dw_rel) || !std::isfinite(st.dp_rel)) {
         c->err = "SIMPLE-like steady solve diverged.";
         return ANB_ERR_DIVERGED;
       }

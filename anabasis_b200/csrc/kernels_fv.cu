@@ -342,7 +342,9 @@ __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
       const double dp = pNew - pOld;
       acc[6] += dp * dp;
       acc[7] += pNew * pNew;
-      acc[8] = fmax(acc[8], fabs(div));
+      // a non-finite divergence must reach the host's divergence test: fmax would drop a NaN
+      const double ad = fabs(div);
+      acc[8] = (ad == ad) ? fmax(acc[8], ad) : INFINITY;
     }
   }
   if (!a.update) return;

@@ -380,10 +380,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld,
   __shared__ double sm[32];
   if (a.fl[0]) return;
   const int n = a.A.n;
-  const double beta = a.fl[3] ? 0.0 : a.sc[2];
+  // first iteration: p = z, and p_old is not read (it may hold anything, NaN included)
+  const bool first = a.fl[3] != 0;
+  const double beta = first ? 0.0 : a.sc[2];
   double acc[1] = {0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const double pr = (double)(T)((double)a.z[r] + beta * (double)pOld[r]);
+    const double pr = first ? (double)a.z[r] : (double)(T)((double)a.z[r] + beta * (double)pOld[r]);
     double q = (double)a.A.diag[r] * pr;
     if constexpr (WM == 0) {
       const int s = r >> 5;
@@ -392,14 +394,15 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld,
       for (int k = 0; k < W; ++k) {
         const int e = b + (k << 5);
         const int c = __ldg(&a.A.col[e]);
-        q += (double)a.A.val[e] * (double)(T)((double)a.z[c] + beta * (double)pOld[c]);
+        q += (double)a.A.val[e] * (first ? (double)a.z[c] : (double)(T)((double)a.z[c] + beta * (double)pOld[c]));
       }
     } else {
       int c[WM];
       double v[WM];
       sell_regs<WM>(a.A.sliceOff, a.A.col, a.A.val, r, c, v);
 #pragma unroll
-      for (int k = 0; k < WM; ++k) q += v[k] * (double)(T)((double)a.z[c[k]] + beta * (double)pOld[c[k]]);
+      for (int k = 0; k < WM; ++k)
+        q += v[k] * (first ? (double)a.z[c[k]] : (double)(T)((double)a.z[c[k]] + beta * (double)pOld[c[k]]));
     }
     pNew[r] = (T)pr;
     a.q[r] = (T)q;
