@@ -113,6 +113,7 @@ void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3
 void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv);
 
 void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
+  ProfScope whole(c->lc, kKfMomentumSolve, 0.0, 0);
   if (c->mixed) return solve_momentum_mixed(c, active, its, conv);
   BicgArgs a{};
   a.A = mom_sell(c);
@@ -187,6 +188,7 @@ PcgArgs pcg_args(anb_ctx* c, const double* b, double* x, double rtol) {
 
 // Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
 void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  ProfScope whole(c->lc, kKfPressureSolve, 0.0, 0);
   if (c->mixed) return solve_pressure_mixed(c, b, x, rtol, its, conv);
   PcgArgs a = pcg_args(c, b, x, rtol);
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
@@ -227,6 +229,10 @@ PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, do
   a.red = c->red;
   return a;
 }
+
+// Coarse levels of at most this many rows run as one cluster kernel (ANB_AMG_TAIL_ROWS overrides;
+// 0 launches every level and sweep separately).  The arithmetic is the same either way.
+constexpr int kAmgTailRows = 1024;
 
 // Aggregation hierarchy for the current level-0 matrix (val0/diag0 on the device, storage type T),
 // coarse levels in T, coarsest inverse in double; the V-cycle is captured as a graph for `ga`.
@@ -278,6 +284,14 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
   A.nDense = nd;
   A.dense = ar.alloc<double>((size_t)nd * nd);
   c->amgBuilt = true;
+  const char* tailEnv = std::getenv("ANB_AMG_TAIL_ROWS");
+  amg_configure_tail(A, tailEnv ? std::atoi(tailEnv) : kAmgTailRows, c->stream);
+  const char* verbose = std::getenv("ANB_AMG_VERBOSE");
+  if (verbose && verbose[0] == '1') {
+    std::fprintf(stderr, "AMG levels:");
+    for (int l = 0; l < A.nLevels; ++l) std::fprintf(stderr, " %d", A.lv[l].n);
+    std::fprintf(stderr, " | tail rows %d, cluster %d\n", A.tailRows, A.tailCluster);
+  }
   const char* noGraph = std::getenv("ANB_NO_GRAPH");
   if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) {
     A.lv[0].b = ga.r;

@@ -12,7 +12,7 @@ namespace anb {
 enum KernelFamily {
   kKfNone = 0, kKfGradient = 1, kKfMomentum = 2, kKfPressureRc = 3, kKfNonOrth = 4, kKfFluxFinal = 5,
   kKfBicgSpmv = 6, kKfPcgSpmv = 7, kKfAmgResid0 = 8, kKfAmgUp0 = 9, kKfAmgCoarse = 10, kKfPcgUpdate = 11,
-  kKfBicgVector = 12, kKfCount = 13
+  kKfBicgVector = 12, kKfMomentumSolve = 13, kKfPressureSolve = 14, kKfCount = 15
 };
 
 // Event-pair recorder for one selected kernel family on one stream.
@@ -271,6 +271,10 @@ struct AmgDevT {
   double corr = 1.6;
   cudaGraphExec_t graph = nullptr;  // captured V-cycle (see amg_capture_graph)
   int graphKernels = 0;
+  // Coarse tail: the CSR levels with at most tailRows rows and the dense level run as one
+  // thread-block-cluster kernel of tailCluster CTAs (0: one launch per level and sweep).
+  int tailRows = 0;
+  int tailCluster = 0;
 };
 using AmgLevelDev = AmgLevelDevT<double>;
 using AmgDev = AmgDevT<double>;
@@ -287,6 +291,10 @@ template <class T>
 void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg);  // Galerkin values + dense inverse
 template <class T>
 cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg);
+// Sets the coarse tail (levels of at most tailRows rows on one cluster; 0 = off) and picks its
+// cluster size for this device.  Call before amg_capture_graph.
+template <class T>
+void amg_configure_tail(AmgDevT<T>& amg, int tailRows, cudaStream_t s);
 
 // ---- mixed-precision defect correction (FP64 outer residual around FP32 inner solves) ------
 // r = b - A x in double with the float matrix, r32 = r, per-component |r|^2 and |b|^2 in

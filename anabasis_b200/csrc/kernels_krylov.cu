@@ -15,10 +15,14 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include <cooperative_groups.h>
+
 #include "kernels.cuh"
 
 namespace anb {
 namespace {
+
+namespace cg = cooperative_groups;
 
 template <class T>
 __device__ __forceinline__ double ld(const T* p) {
@@ -476,10 +480,24 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
   }
 }
 
+constexpr int kCoarseLanes = 8;  // lanes per row on the CSR coarse levels
+
+// Vector loads of the coarse sweeps: the read-only path for vectors written by earlier launches,
+// the L2 path for vectors written earlier in the same launch (the cluster tail below).
+struct LdRO {
+  template <class T>
+  __device__ __forceinline__ double operator()(const T* p) const { return (double)__ldg(p); }
+};
+struct LdL2 {
+  template <class T>
+  __device__ __forceinline__ double operator()(const T* p) const { return (double)__ldcg(p); }
+};
+
 // Coarse levels (CSR): G consecutive lanes share one row, each lane takes every G-th entry, and
 // the partial sums meet through warp shuffles.  Coarse rows are long and there are few of them,
 // so splitting rows keeps enough loads in flight.  The warp-level loop bound keeps every lane of
-// a warp in the shuffles.
+// a warp in the shuffles.  The row sweeps are device functions over (warp, nWarps) so that the
+// per-level kernels and the cluster tail run the same arithmetic.
 template <int G>
 __device__ __forceinline__ double group_sum(double v) {
 #pragma unroll
@@ -487,13 +505,11 @@ __device__ __forceinline__ double group_sum(double v) {
   return v;
 }
 
-template <int G, class T>
-__global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLevelDevT<T> f, double omega) {
-  if (*done) return;
+// Down, part 1 on a CSR level: x = w D^-1 b, x2 = b - A x.
+template <int G, class T, class LD>
+__device__ __forceinline__ void resid_csr_rows(const AmgLevelDevT<T>& f, int warp, int nWarps, LD ldv) {
   const int lane = threadIdx.x & 31, sub = lane % G;
   const int rowsPerWarp = 32 / G;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int base = warp * rowsPerWarp; base < f.n; base += nWarps * rowsPerWarp) {
     const int i = base + lane / G;
     double acc = 0.0;
@@ -501,12 +517,12 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLe
       const int k1 = __ldg(&f.rowOff[i + 1]);
       for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
         const int j = __ldg(&f.col[k]);
-        acc += ld(&f.val[k]) * (ld(&f.wdinv[j]) * ld(&f.b[j]));
+        acc += ld(&f.val[k]) * (ld(&f.wdinv[j]) * ldv(&f.b[j]));
       }
     }
     acc = group_sum<G>(acc);
     if (i < f.n && sub == 0) {
-      const double di = ld(&f.diag[i]), bi = ld(&f.b[i]);
+      const double di = ld(&f.diag[i]), bi = ldv(&f.b[i]);
       const double xi = ld(&f.wdinv[i]) * bi;
       f.x[i] = (T)xi;
       f.x2[i] = (T)(bi - di * xi - acc);
@@ -514,14 +530,12 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLe
   }
 }
 
-template <int G, class T>
-__global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevelDevT<T> f, const T* e, double omega,
-                                                       double corr, T* out) {
-  if (*done) return;
+// Up on a CSR level: out = xt + w D^-1 (b - A xt) with xt = x + corr e[agg].
+template <int G, class T, class LD>
+__device__ __forceinline__ void up_csr_rows(const AmgLevelDevT<T>& f, const T* e, double corr, T* out, int warp,
+                                            int nWarps, LD ldv) {
   const int lane = threadIdx.x & 31, sub = lane % G;
   const int rowsPerWarp = 32 / G;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
   for (int base = warp * rowsPerWarp; base < f.n; base += nWarps * rowsPerWarp) {
     const int i = base + lane / G;
     double acc = 0.0;
@@ -529,29 +543,62 @@ __global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevel
       const int k1 = __ldg(&f.rowOff[i + 1]);
       for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
         const int j = __ldg(&f.col[k]);
-        acc += ld(&f.val[k]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
+        acc += ld(&f.val[k]) * (ldv(&f.x[j]) + corr * ldv(&e[__ldg(&f.agg[j])]));
       }
     }
     acc = group_sum<G>(acc);
     if (i < f.n && sub == 0) {
       const double di = ld(&f.diag[i]);
-      const double xi = ld(&f.x[i]) + corr * ld(&e[__ldg(&f.agg[i])]);
-      out[i] = (T)(xi + ld(&f.wdinv[i]) * (ld(&f.b[i]) - di * xi - acc));
+      const double xi = ldv(&f.x[i]) + corr * ldv(&e[__ldg(&f.agg[i])]);
+      out[i] = (T)(xi + ld(&f.wdinv[i]) * (ldv(&f.b[i]) - di * xi - acc));
     }
   }
 }
 
-// Down, part 2: piecewise-constant restriction b_next[I] = sum of r over the rows of I.
-template <class T>
-__global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLevelDevT<T> f, T* bNext) {
-  if (*done) return;
-  for (int I = blockIdx.x * blockDim.x + threadIdx.x; I < f.nc; I += gridDim.x * blockDim.x) {
+// Down, part 2: piecewise-constant restriction b_next[I] = sum of r over the rows of I
+// (thread t of nT).
+template <class T, class LD>
+__device__ __forceinline__ void restrict_rows(const AmgLevelDevT<T>& f, T* bNext, int t, int nT, LD ldv) {
+  for (int I = t; I < f.nc; I += nT) {
     double acc = 0.0;
     const int m1 = __ldg(&f.memOff[I + 1]);
 #pragma unroll 4
-    for (int mm = __ldg(&f.memOff[I]); mm < m1; ++mm) acc += (double)f.x2[__ldg(&f.mem[mm])];
+    for (int mm = __ldg(&f.memOff[I]); mm < m1; ++mm) acc += ldv(&f.x2[__ldg(&f.mem[mm])]);
     bNext[I] = (T)acc;
   }
+}
+
+// Coarsest level: x = A^-1 b with the stored dense inverse (double), warp per row, lanes across
+// the row (coalesced).
+template <class T, class LD>
+__device__ __forceinline__ void dense_rows(int n, const double* inv, const T* b, T* x, int warp, int nWarps, LD ldv) {
+  const int lane = threadIdx.x & 31;
+  for (int i = warp; i < n; i += nWarps) {
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += __ldg(&inv[(size_t)i * n + j]) * ldv(&b[j]);
+    s = warp_sum(s);
+    if (lane == 0) x[i] = (T)s;
+  }
+}
+
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLevelDevT<T> f, double omega) {
+  if (*done) return;
+  resid_csr_rows<G>(f, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, (gridDim.x * blockDim.x) >> 5, LdRO{});
+}
+
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_amg_up_csr(const int* done, AmgLevelDevT<T> f, const T* e, double omega,
+                                                       double corr, T* out) {
+  if (*done) return;
+  up_csr_rows<G>(f, e, corr, out, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, (gridDim.x * blockDim.x) >> 5,
+                 LdRO{});
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLevelDevT<T> f, T* bNext) {
+  if (*done) return;
+  restrict_rows(f, bNext, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, LdRO{});
 }
 
 // Up: prolongate the coarse correction and post-smooth (one weighted-Jacobi sweep) in one pass:
@@ -601,16 +648,47 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
   }
 }
 
-// Coarsest level: x = A^-1 b with the stored dense inverse (double, one block), warp per row.
+// Coarsest level on its own: one block.
 template <class T>
 __global__ void k_amg_dense_apply(const int* done, int n, const double* inv, const T* b, T* x) {
   if (*done) return;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int i = w; i < n; i += nw) {  // lanes across the row (coalesced)
-    double s = 0.0;
-    for (int j = lane; j < n; j += 32) s += __ldg(&inv[(size_t)i * n + j]) * ld(&b[j]);
-    s = warp_sum(s);
-    if (lane == 0) x[i] = (T)s;
+  dense_rows(n, inv, b, x, threadIdx.x >> 5, blockDim.x >> 5, LdRO{});
+}
+
+// The coarse tail of the V-cycle in one launch: levels lv[0..nLev-2] (CSR) down, the dense
+// level lv[nLev-1], and the same levels up, on one thread-block cluster whose barriers order the
+// sweeps.  Every sweep is the per-level kernels' arithmetic; vectors written inside the launch
+// are read through L2.  All CTAs of the cluster take the same barriers (the loop bounds and the
+// done flag are uniform), so each barrier completes.
+constexpr int kTailThreads = 1024;
+constexpr int kTailMaxLevels = 12;
+template <class T>
+struct AmgTailArgs {
+  int nLev;
+  AmgLevelDevT<T> lv[kTailMaxLevels];
+  const double* dense;
+  double corr;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_amg_tail(const int* done, const __grid_constant__ AmgTailArgs<T> a) {
+  if (*done) return;
+  cg::cluster_group cl = cg::this_cluster();
+  const int t = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+  const int nT = (int)cl.num_blocks() * blockDim.x;
+  const int warp = t >> 5, nWarps = nT >> 5;
+  const int L = a.nLev;
+  for (int l = 0; l + 1 < L; ++l) {
+    resid_csr_rows<kCoarseLanes>(a.lv[l], warp, nWarps, LdL2{});
+    cl.sync();
+    restrict_rows(a.lv[l], a.lv[l + 1].b, t, nT, LdL2{});
+    cl.sync();
+  }
+  dense_rows(a.lv[L - 1].n, a.dense, a.lv[L - 1].b, a.lv[L - 1].x, warp, nWarps, LdL2{});
+  for (int l = L - 2; l >= 0; --l) {
+    cl.sync();
+    const T* e = (l + 1 == L - 1) ? a.lv[l + 1].x : a.lv[l + 1].x2;
+    up_csr_rows<kCoarseLanes>(a.lv[l], e, a.corr, a.lv[l].x2, warp, nWarps, LdL2{});
   }
 }
 
@@ -776,7 +854,63 @@ void pcg_init(const LaunchCfg& lc, const PcgArgsT<T>& a) {
 
 static int blocks_for(int n, int cap) { return std::max(1, std::min(cap, (n + kBlock - 1) / kBlock)); }
 
-constexpr int kCoarseLanes = 8;  // lanes per row on the CSR coarse levels
+// First level of the cluster tail; L - 1 (the dense level alone, no tail) when the tail is off or
+// no CSR level is small enough.  Level sizes fall with depth, so the tail is a suffix.
+template <class T>
+static int tail_start(const AmgDevT<T>* amg) {
+  const int L = amg->nLevels;
+  if (amg->tailCluster <= 0 || amg->tailRows <= 0) return L - 1;
+  int t0 = L - 1;
+  while (t0 - 1 >= 1 && amg->lv[t0 - 1].n <= amg->tailRows && L - (t0 - 1) <= kTailMaxLevels) --t0;
+  return t0;
+}
+
+static cudaLaunchConfig_t tail_config(cudaStream_t s, int cluster, cudaLaunchAttribute* at) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(cluster);
+  cfg.blockDim = dim3(kTailThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cluster;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <class T>
+static void launch_tail(const LaunchCfg& lc, const int* done, const AmgDevT<T>* amg, int t0) {
+  AmgTailArgs<T> ta{};
+  ta.nLev = amg->nLevels - t0;
+  for (int l = 0; l < ta.nLev; ++l) ta.lv[l] = amg->lv[t0 + l];
+  ta.dense = amg->dense;
+  ta.corr = amg->corr;
+  cudaLaunchAttribute at[1];
+  const cudaLaunchConfig_t cfg = tail_config(lc.stream, amg->tailCluster, at);
+  cudaLaunchKernelEx(&cfg, k_amg_tail<T>, done, ta);
+}
+
+// Cluster size of the tail: 16 CTAs (a non-portable size) when the device can co-schedule them,
+// else 8; 0 (no tail) when neither fits.
+template <class T>
+void amg_configure_tail(AmgDevT<T>& amg, int tailRows, cudaStream_t s) {
+  amg.tailRows = tailRows;
+  amg.tailCluster = 0;
+  if (tailRows <= 0) return;
+  cudaFuncSetAttribute(k_amg_tail<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  for (int cs : {16, 8}) {
+    cudaLaunchAttribute at[1];
+    const cudaLaunchConfig_t cfg = tail_config(s, cs, at);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_amg_tail<T>, &cfg) == cudaSuccess && n > 0) {
+      amg.tailCluster = cs;
+      return;
+    }
+    cudaGetLastError();
+  }
+}
 
 template <class T>
 static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
@@ -793,16 +927,21 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
-    ProfScope ps(lc, kKfAmgCoarse, 0.0, 3 * L - 6);
-    for (int l = 1; l + 1 < L; ++l) {
+    const int t0 = tail_start(amg);
+    ProfScope ps(lc, kKfAmgCoarse, 0.0, 3 * (t0 - 1) + 1);
+    for (int l = 1; l < t0; ++l) {
       const AmgLevelDevT<T>& f = amg->lv[l];
       k_amg_resid_csr<kCoarseLanes, T><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, amg->omega);
       k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
     }
-    const AmgLevelDevT<T>& c = amg->lv[L - 1];
-    k_amg_dense_apply<T><<<1, 1024, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
-    for (int l = L - 2; l >= 1; --l) {
+    if (t0 < L - 1) {
+      launch_tail(lc, a.fl, amg, t0);
+    } else {
+      const AmgLevelDevT<T>& c = amg->lv[L - 1];
+      k_amg_dense_apply<T><<<1, 1024, 0, lc.stream>>>(a.fl, c.n, amg->dense, c.b, c.x);
+    }
+    for (int l = t0 - 1; l >= 1; --l) {
       const AmgLevelDevT<T>& f = amg->lv[l];
       // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
       const T* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
@@ -914,7 +1053,8 @@ void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, floa
   template void pcg_iteration<T>(const LaunchCfg&, const PcgArgsT<T>&, int, const AmgDevT<T>*); \
   template void pcg_precondition<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*);  \
   template void amg_refresh<T>(const LaunchCfg&, AmgDevT<T>&);                                \
-  template cudaError_t amg_capture_graph<T>(const LaunchCfg&, const PcgArgsT<T>&, AmgDevT<T>&);
+  template cudaError_t amg_capture_graph<T>(const LaunchCfg&, const PcgArgsT<T>&, AmgDevT<T>&);           \
+  template void amg_configure_tail<T>(AmgDevT<T>&, int, cudaStream_t);
 ANB_INSTANTIATE(double)
 ANB_INSTANTIATE(float)
 #undef ANB_INSTANTIATE

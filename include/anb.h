@@ -241,6 +241,13 @@ int anb_debug_vjp(anb_ctx* ctx, const double* w, double* out, double* gbc, doubl
 #define ANB_KF_FLUX_FINAL 5    /* flux/velocity correction           */
 #define ANB_KF_BICG_SPMV 6     /* BiCGSTAB matrix-vector products    */
 #define ANB_KF_PCG_SPMV 7      /* PCG matrix-vector product          */
+#define ANB_KF_AMG_RESID0 8    /* V-cycle level 0 down sweep + restriction (ungraphed V-cycles) */
+#define ANB_KF_AMG_UP0 9       /* V-cycle level 0 up sweep (ungraphed V-cycles)               */
+#define ANB_KF_AMG_COARSE 10   /* V-cycle coarse levels (ungraphed V-cycles)                  */
+#define ANB_KF_PCG_UPDATE 11   /* PCG x, r update and residual norm                           */
+#define ANB_KF_BICG_VECTOR 12  /* BiCGSTAB vector updates                                     */
+#define ANB_KF_MOMENTUM_SOLVE 13 /* whole momentum solve, host polls included                 */
+#define ANB_KF_PRESSURE_SOLVE 14 /* whole pressure solve, host polls included                 */
 int anb_profile_select(anb_ctx* ctx, int family);
 int anb_profile_read(anb_ctx* ctx, long long* launches, double* seconds, double* algo_bytes);
 /* Number of kernel launches this process has issued through libanb.so. */
