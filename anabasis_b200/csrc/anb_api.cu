@@ -825,6 +825,22 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     dm.slotFace = A.upload(L.slotFace);
     dm.face = c->dFace;
     dm.fFlags = A.upload(L.fFlags);
+    {
+      const size_t nE = (size_t)c->nEnt;
+      std::vector<double> sg(8 * nE, 0.0);
+      std::vector<uint8_t> sf(nE, 0);
+      for (size_t e = 0; e < nE; ++e) {
+        const int f = L.slotFace[e];
+        if (f < 0) continue;
+        const FaceRec& r = fr[f];
+        const double v[8] = {r.lam, r.g, r.t[0], r.t[1], r.t[2], r.d[0], r.d[1], r.d[2]};
+        for (int q = 0; q < 8; ++q) sg[q * nE + e] = v[q];
+        sf[e] = L.fFlags[f];
+      }
+      dm.nEnt = c->nEnt;
+      dm.slotGeom = A.upload(sg);
+      dm.slotFlags = A.upload(sf);
+    }
     dm.bOwner = A.upload(L.bOwner);
     dm.bnd = c->dBnd;
     dm.bFlags = A.upload(L.bFlags);

@@ -33,6 +33,12 @@ struct DMesh {
   const int* slotFace;
   const FaceRec* face;
   const uint8_t* fFlags;
+  // the face record of every slot, copied into slot order as 8 arrays of nEnt doubles (lam, g,
+  // t[3], d[3]; zero on padding) with the face flags per slot: the slot loop of a warp then reads
+  // its faces' geometry as contiguous runs instead of gathering 64-byte records by face index
+  int nEnt;
+  const double* slotGeom;
+  const uint8_t* slotFlags;
   const int* bOwner;
   const BndRec* bnd;
   const uint8_t* bFlags;
@@ -58,6 +64,20 @@ __device__ __forceinline__ void load_face(const FaceRec* F, int f, double& lam, 
   const double2* p = reinterpret_cast<const double2*>(F + f);
   const double2 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), e = __ldg(p + 3);
   lam = a.x; g = a.y; t[0] = b.x; t[1] = b.y; t[2] = c.x; d[0] = c.y; d[1] = e.x; d[2] = e.y;
+}
+
+// Face geometry of storage slot e (owner orientation, as in FaceRec).
+__device__ __forceinline__ void load_slot(const DMesh& m, int e, double& lam, double& g, double t[3], double d[3]) {
+  const double* s = m.slotGeom + e;
+  const size_t n = (size_t)m.nEnt;
+  lam = __ldg(s);
+  g = __ldg(s + n);
+  t[0] = __ldg(s + 2 * n);
+  t[1] = __ldg(s + 3 * n);
+  t[2] = __ldg(s + 4 * n);
+  d[0] = __ldg(s + 5 * n);
+  d[1] = __ldg(s + 6 * n);
+  d[2] = __ldg(s + 7 * n);
 }
 
 __device__ __forceinline__ void load_bnd(const BndRec* B, int b, double& g, double t[3], double S[3], double d[3]) {

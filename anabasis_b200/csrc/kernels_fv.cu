@@ -16,7 +16,6 @@ template <int NF>
 __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
   const int C = m.nCells;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
-    const double xr0 = m.cc[3 * r], xr1 = m.cc[3 * r + 1], xr2 = m.cc[3 * r + 2];
     double pr[NF], b[NF][3];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
@@ -29,7 +28,11 @@ __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
       const int e = base + (k << 5);
       if (__ldg(&m.slotFace[e]) < 0) break;
       const int c = __ldg(&m.col[e]);
-      const double r0 = __ldg(&m.cc[3 * c]) - xr0, r1 = __ldg(&m.cc[3 * c + 1]) - xr1, r2 = __ldg(&m.cc[3 * c + 2]) - xr2;
+      // cc_c - cc_r: the slot's d (cc_N - cc_P) with the sign of the row's side, bit for bit
+      const double sgn = r < c ? 1.0 : -1.0;
+      const size_t n = (size_t)m.nEnt;
+      const double r0 = sgn * __ldg(&m.slotGeom[5 * n + e]), r1 = sgn * __ldg(&m.slotGeom[6 * n + e]),
+                   r2 = sgn * __ldg(&m.slotGeom[7 * n + e]);
       const double w = 1.0 / fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-30);
 #pragma unroll
       for (int f = 0; f < NF; ++f) {
@@ -92,14 +95,14 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
         if (full) a.val[e] = M(0);
         continue;
       }
-      if (!(__ldg(&m.fFlags[f]) & 1)) {
+      if (!(__ldg(&m.slotFlags[e]) & 1)) {
         if (full) a.val[e] = M(0);
         continue;
       }
       const int c = __ldg(&m.col[e]);
       const bool own = r < c;
       double lam, g, t[3], d[3];
-      load_face(m.face, f, lam, g, t, d);
+      load_slot(m, e, lam, g, t, d);
       const int P = own ? r : c, N = own ? c : r;
       const double l1 = 1.0 - lam;
       const double alpha = mu * g;
@@ -191,11 +194,11 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a)
       const int c = __ldg(&m.col[e]);
       const bool own = r < c;
       double lam, g, t[3], d[3];
-      load_face(m.face, f, lam, g, t, d);
+      load_slot(m, e, lam, g, t, d);
       const int P = own ? r : c, N = own ? c : r;
       const double l1 = 1.0 - lam;
       const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
-      if (__ldg(&m.fFlags[f]) & 1) {
+      if (__ldg(&m.slotFlags[e]) & 1) {
         const double coeff = g * rAUf;
         a.val[e] = (M)(-coeff);
         pd += coeff;
@@ -250,11 +253,11 @@ __global__ void __launch_bounds__(kBlock) k_nonorth_rhs(DMesh m, NonOrthArgs a) 
       const int e = base + (k << 5);
       const int f = __ldg(&m.slotFace[e]);
       if (f < 0) break;
-      if (!(__ldg(&m.fFlags[f]) & 2)) continue;
+      if (!(__ldg(&m.slotFlags[e]) & 2)) continue;
       const int c = __ldg(&m.col[e]);
       const bool own = r < c;
       double lam, g, t[3], d[3];
-      load_face(m.face, f, lam, g, t, d);
+      load_slot(m, e, lam, g, t, d);
       const int P = own ? r : c, N = own ? c : r;
       const double l1 = 1.0 - lam;
       const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
@@ -293,12 +296,12 @@ __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
       const int c = __ldg(&m.col[e]);
       const bool own = r < c;
       double lam, g, t[3], d[3];
-      load_face(m.face, f, lam, g, t, d);
+      load_slot(m, e, lam, g, t, d);
       const int P = own ? r : c, N = own ? c : r;
       const double l1 = 1.0 - lam;
       const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
       double phiNO = 0.0;
-      if (__ldg(&m.fFlags[f]) & 2) {
+      if (__ldg(&m.slotFlags[e]) & 2) {
         const double gx = l1 * Gc[P] + lam * Gc[N], gy = l1 * Gc[C + P] + lam * Gc[C + N],
                      gz = l1 * Gc[2 * C + P] + lam * Gc[2 * C + N];
         phiNO = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
