@@ -820,6 +820,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     dm.nInternal = c->nI;
     dm.nBoundary = c->nB;
     dm.nSlices = L.nSlices;
+    dm.maxW = L.maxRowLen;
     dm.sliceOff = A.upload(L.sliceOff);
     dm.col = A.upload(L.col);
     dm.slotFace = A.upload(L.slotFace);

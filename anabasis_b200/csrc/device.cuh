@@ -28,6 +28,7 @@ struct __align__(16) BndRec {
 // Read-only mesh view passed by value to kernels.
 struct DMesh {
   int nCells, nInternal, nBoundary, nSlices;
+  int maxW;             // largest slice width (slots per row)
   const int* sliceOff;
   const int* col;
   const int* slotFace;

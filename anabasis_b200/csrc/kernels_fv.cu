@@ -11,35 +11,69 @@ namespace anb {
 
 namespace {
 
+// Slot indices of row r in registers for a compile-time bound WM on the slice width (slots past
+// the row's width read as face -1, column r), so every load of the slot loop below can be issued
+// before the first result is needed.  Returns the row's first storage index.
+template <int WM>
+__device__ __forceinline__ int slot_regs(const DMesh& m, int r, int (&f)[WM], int (&c)[WM]) {
+  const int s = r >> 5;
+  const int b0 = __ldg(&m.sliceOff[s]);
+  const int W = (__ldg(&m.sliceOff[s + 1]) - b0) >> 5;
+  const int base = b0 + (r & 31);
+#pragma unroll
+  for (int k = 0; k < WM; ++k) {
+    f[k] = -1;
+    c[k] = r;
+    if (k < W) {
+      f[k] = __ldg(&m.slotFace[base + (k << 5)]);
+      c[k] = __ldg(&m.col[base + (k << 5)]);
+    }
+  }
+  return base;
+}
+
 // ---- least-squares gradient: main.cu:1403-1440 on the moments of main.cu:1159-1251 ----------
 template <int NF>
+__device__ __forceinline__ void grad_slot(const DMesh& m, const GradArgs& a, int r, int e, int c,
+                                          const double (&pr)[NF], double (&b)[NF][3]) {
+  // cc_c - cc_r: the slot's d (cc_N - cc_P) with the sign of the row's side, bit for bit
+  const double sgn = r < c ? 1.0 : -1.0;
+  const size_t n = (size_t)m.nEnt;
+  const double r0 = sgn * __ldg(&m.slotGeom[5 * n + e]), r1 = sgn * __ldg(&m.slotGeom[6 * n + e]),
+               r2 = sgn * __ldg(&m.slotGeom[7 * n + e]);
+  const double w = 1.0 / fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-30);
+#pragma unroll
+  for (int f = 0; f < NF; ++f) {
+    const double dp = w * (__ldg(&a.phi[f][c]) - pr[f]);
+    b[f][0] += r0 * dp;
+    b[f][1] += r1 * dp;
+    b[f][2] += r2 * dp;
+  }
+}
+
+template <int NF, int WM>
 __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
   const int C = m.nCells;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
     double pr[NF], b[NF][3];
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
-      pr[f] = a.phi[f][r];
+      pr[f] = __ldg(&a.phi[f][r]);
       b[f][0] = b[f][1] = b[f][2] = 0.0;
     }
-    int W;
-    const int base = row_base(m, r, W);
-    for (int k = 0; k < W; ++k) {
-      const int e = base + (k << 5);
-      if (__ldg(&m.slotFace[e]) < 0) break;
-      const int c = __ldg(&m.col[e]);
-      // cc_c - cc_r: the slot's d (cc_N - cc_P) with the sign of the row's side, bit for bit
-      const double sgn = r < c ? 1.0 : -1.0;
-      const size_t n = (size_t)m.nEnt;
-      const double r0 = sgn * __ldg(&m.slotGeom[5 * n + e]), r1 = sgn * __ldg(&m.slotGeom[6 * n + e]),
-                   r2 = sgn * __ldg(&m.slotGeom[7 * n + e]);
-      const double w = 1.0 / fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-30);
+    if constexpr (WM > 0) {
+      int fs[WM], cs[WM];
+      const int base = slot_regs<WM>(m, r, fs, cs);
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        const double dp = w * (a.phi[f][c] - pr[f]);
-        b[f][0] += r0 * dp;
-        b[f][1] += r1 * dp;
-        b[f][2] += r2 * dp;
+      for (int k = 0; k < WM; ++k)
+        if (fs[k] >= 0) grad_slot<NF>(m, a, r, base + (k << 5), cs[k], pr, b);
+    } else {
+      int W;
+      const int base = row_base(m, r, W);
+      for (int k = 0; k < W; ++k) {
+        const int e = base + (k << 5);
+        if (__ldg(&m.slotFace[e]) < 0) break;
+        grad_slot<NF>(m, a, r, e, __ldg(&m.col[e]), pr, b);
       }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
@@ -72,12 +106,49 @@ __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
 
 // ---- momentum: K25,K4,K2,K3,K5,K6 + rhs-only K26,K9,K7,K8,K10 for V and W in one pass ------
 // main.cu:1678-1896 (assembly), 1686-1695 (relaxation), 1787-1802 (rAU), loop 3350-3405.
+// Contributions of internal slot e (neighbour c) of row r: the off-diagonal value, and the
+// diagonal and right-hand-side increments of the row.  Row values (U, the 9 velocity-gradient
+// components) come in registers; owner-orientation P/N values are selected, not re-loaded, so
+// the arithmetic is that of a face visited from either side.
 template <class M>
+__device__ __forceinline__ void momentum_slot(const DMesh& m, const MomArgsT<M>& a, int C, int r, int e, int c,
+                                              const double (&ur)[3], const double (&gr)[9], double& val,
+                                              double& dDiag, double (&dRhs)[3]) {
+  const bool own = r < c;
+  double lam, g, t[3], d[3];
+  load_slot(m, e, lam, g, t, d);
+  const double l1 = 1.0 - lam;
+  const double alpha = a.mu * g;
+  const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
+  double uc[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const double x = __ldg(&a.U[q * C + c]);
+    uc[q] = l1 * (own ? ur[q] : x) + lam * (own ? x : ur[q]);
+  }
+  const double F = a.rho * (uc[0] * S0 + uc[1] * S1 + uc[2] * S2);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double gq[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double x = __ldg(&a.G[(3 * q + k) * C + c]);
+      gq[k] = l1 * (own ? gr[3 * q + k] : x) + lam * (own ? x : gr[3 * q + k]);
+    }
+    dRhs[q] = a.mu * (gq[0] * t[0] + gq[1] * t[1] + gq[2] * t[2]);
+  }
+  if (own) {
+    val = -alpha + F * lam;
+    dDiag = alpha + F * l1;
+  } else {
+    val = -alpha - F * l1;
+    dDiag = alpha - F * lam;
+  }
+}
+
+template <class M, int WM>
 __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
   const int C = m.nCells;
-  const double* U0 = a.U;
-  const double* U1 = a.U + C;
-  const double* U2 = a.U + 2 * C;
   const bool full = !a.rhsOnly;
   const double* G = a.G;
   const double rho = a.rho, mu = a.mu;
@@ -85,46 +156,46 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
     const double V = m.vol[r];
     double rhs0 = -G[9 * C + r] * V, rhs1 = -G[10 * C + r] * V, rhs2 = -G[11 * C + r] * V;
     double diag = 0.0;
-    const double ur0 = U0[r], ur1 = U1[r], ur2 = U2[r];
-    int W;
-    const int base = row_base(m, r, W);
-    for (int k = 0; k < W; ++k) {
-      const int e = base + (k << 5);
-      const int f = __ldg(&m.slotFace[e]);
-      if (f < 0) {
-        if (full) a.val[e] = M(0);
-        continue;
-      }
-      if (!(__ldg(&m.slotFlags[e]) & 1)) {
-        if (full) a.val[e] = M(0);
-        continue;
-      }
-      const int c = __ldg(&m.col[e]);
-      const bool own = r < c;
-      double lam, g, t[3], d[3];
-      load_slot(m, e, lam, g, t, d);
-      const int P = own ? r : c, N = own ? c : r;
-      const double l1 = 1.0 - lam;
-      const double alpha = mu * g;
-      const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
-      const double uc0 = l1 * U0[P] + lam * U0[N], uc1 = l1 * U1[P] + lam * U1[N], uc2 = l1 * U2[P] + lam * U2[N];
-      const double F = rho * (uc0 * S0 + uc1 * S1 + uc2 * S2);
-      double corr[3];
+    const double ur[3] = {__ldg(&a.U[r]), __ldg(&a.U[C + r]), __ldg(&a.U[2 * C + r])};
+    double gr[9];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const double* gq = G + 3 * q * C;
-        const double gx = l1 * gq[P] + lam * gq[N], gy = l1 * gq[C + P] + lam * gq[C + N],
-                     gz = l1 * gq[2 * C + P] + lam * gq[2 * C + N];
-        corr[q] = mu * (gx * t[0] + gy * t[1] + gz * t[2]);
-      }
-      if (own) {
-        if (full) a.val[e] = (M)(-alpha + F * lam);
-        diag += alpha + F * l1;
-        rhs0 += corr[0]; rhs1 += corr[1]; rhs2 += corr[2];
+    for (int k = 0; k < 9; ++k) gr[k] = __ldg(&G[k * C + r]);
+    auto add = [&](int e, int c, double& val) {
+      double dd, dr[3];
+      momentum_slot(m, a, C, r, e, c, ur, gr, val, dd, dr);
+      diag += dd;
+      if (r < c) {
+        rhs0 += dr[0]; rhs1 += dr[1]; rhs2 += dr[2];
       } else {
-        if (full) a.val[e] = (M)(-alpha - F * l1);
-        diag += alpha - F * lam;
-        rhs0 -= corr[0]; rhs1 -= corr[1]; rhs2 -= corr[2];
+        rhs0 -= dr[0]; rhs1 -= dr[1]; rhs2 -= dr[2];
+      }
+    };
+    if constexpr (WM > 0) {
+      // every load of the row first, the matrix stores after the loop
+      int fs[WM], cs[WM];
+      const int base = slot_regs<WM>(m, r, fs, cs);
+      double vals[WM];
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        vals[k] = 0.0;
+        if (fs[k] < 0 || !(__ldg(&m.slotFlags[base + (k << 5)]) & 1)) continue;
+        add(base + (k << 5), cs[k], vals[k]);
+      }
+      if (full) {
+        const int W = (__ldg(&m.sliceOff[(r >> 5) + 1]) - __ldg(&m.sliceOff[r >> 5])) >> 5;
+#pragma unroll
+        for (int k = 0; k < WM; ++k)
+          if (k < W) a.val[base + (k << 5)] = (M)vals[k];
+      }
+    } else {
+      int W;
+      const int base = row_base(m, r, W);
+      for (int k = 0; k < W; ++k) {
+        const int e = base + (k << 5);
+        const int f = __ldg(&m.slotFace[e]);
+        double v = 0.0;
+        if (f >= 0 && (__ldg(&m.slotFlags[e]) & 1)) add(e, __ldg(&m.col[e]), v);
+        if (full) a.val[e] = (M)v;
       }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
@@ -136,12 +207,12 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
       const unsigned ty = __ldg(&m.bType[bf]);
       const double alpha = mu * g;
       const double bu = m.bVal[bf], bv = m.bVal[m.nBoundary + bf], bw = m.bVal[2 * m.nBoundary + bf];
-      const double ub = (ty & 1u) ? bu : ur0, vb = (ty & 2u) ? bv : ur1, wb = (ty & 4u) ? bw : ur2;
+      const double ub = (ty & 1u) ? bu : ur[0], vb = (ty & 2u) ? bv : ur[1], wb = (ty & 4u) ? bw : ur[2];
       const double F = rho * (ub * S[0] + vb * S[1] + wb * S[2]);
       diag += (ty & 1u) ? alpha : F;  // the matrix carries the u-component BC types
-      if (ty & 1u) rhs0 += alpha * bu + mu * (G[r] * t[0] + G[C + r] * t[1] + G[2 * C + r] * t[2]) - F * bu;
-      if (ty & 2u) rhs1 += alpha * bv + mu * (G[3 * C + r] * t[0] + G[4 * C + r] * t[1] + G[5 * C + r] * t[2]) - F * bv;
-      if (ty & 4u) rhs2 += alpha * bw + mu * (G[6 * C + r] * t[0] + G[7 * C + r] * t[1] + G[8 * C + r] * t[2]) - F * bw;
+      if (ty & 1u) rhs0 += alpha * bu + mu * (gr[0] * t[0] + gr[1] * t[1] + gr[2] * t[2]) - F * bu;
+      if (ty & 2u) rhs1 += alpha * bv + mu * (gr[3] * t[0] + gr[4] * t[1] + gr[5] * t[2]) - F * bv;
+      if (ty & 4u) rhs2 += alpha * bw + mu * (gr[6] * t[0] + gr[7] * t[1] + gr[8] * t[2]) - F * bw;
     }
     const double q0 = a.Q[r], q1 = a.Q[C + r], q2 = a.Q[2 * C + r];
     if (full) {
@@ -171,52 +242,106 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
 
 // ---- pressure matrix (K11,K12) + Rhie-Chow flux (K14) + continuity (K15) ------------------
 // main.cu:1898-1950, 1474-1536, launch sequence 3407-3452.
+// Internal slot e (neighbour c) of row r: the pressure coefficient g rAU_f (returned through
+// coeff) and the Rhie-Chow flux in owner orientation, equal bit for bit from both sides.  Row
+// values come in registers.
+struct PresRow {
+  double rau, u[3], gp[3], p;
+};
 template <class M>
+__device__ __forceinline__ double prc_slot(const DMesh& m, const PresArgsT<M>& a, int C, int r, int e, int c,
+                                           const PresRow& R, double& coeff) {
+  const bool own = r < c;
+  double lam, g, t[3], d[3];
+  load_slot(m, e, lam, g, t, d);
+  const double l1 = 1.0 - lam;
+  const double rc_ = __ldg(&a.rau[c]);
+  const double rAUf = l1 * (own ? R.rau : rc_) + lam * (own ? rc_ : R.rau);
+  coeff = g * rAUf;
+  const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
+  double uf[3], gf[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const double x = __ldg(&a.Us[q * C + c]);
+    uf[q] = l1 * (own ? R.u[q] : x) + lam * (own ? x : R.u[q]);
+    const double y = __ldg(&a.Gp[q * C + c]);
+    gf[q] = l1 * (own ? R.gp[q] : y) + lam * (own ? y : R.gp[q]);
+  }
+  const double pc_ = __ldg(&a.P[c]);
+  const double pP = own ? R.p : pc_, pN = own ? pc_ : R.p;
+  const double phiI = a.rho * (uf[0] * S0 + uf[1] * S1 + uf[2] * S2);
+  const double rc = a.rho * g * rAUf * ((pN - pP) - (gf[0] * d[0] + gf[1] * d[1] + gf[2] * d[2]));
+  return phiI - rc;
+}
+
+template <class M, int WM>
 __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a) {
   const int C = m.nCells, nI = m.nInternal;
-  const double* U0 = a.Us;
-  const double* U1 = a.Us + C;
-  const double* U2 = a.Us + 2 * C;
-  const double* Gp = a.Gp;
   const double rho = a.rho;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
     double pd = 0.0, div = 0.0;
-    const double rAUr = a.rau[r];
-    int W;
-    const int base = row_base(m, r, W);
-    for (int k = 0; k < W; ++k) {
-      const int e = base + (k << 5);
-      const int f = __ldg(&m.slotFace[e]);
-      if (f < 0) {
-        a.val[e] = M(0);
-        continue;
+    PresRow R;
+    R.rau = __ldg(&a.rau[r]);
+    R.p = __ldg(&a.P[r]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      R.u[q] = __ldg(&a.Us[q * C + r]);
+      R.gp[q] = __ldg(&a.Gp[q * C + r]);
+    }
+    if constexpr (WM > 0) {
+      // every load of the row first, the stores after the loop
+      int fs[WM], cs[WM];
+      const int base = slot_regs<WM>(m, r, fs, cs);
+      double vals[WM], ph[WM];
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        vals[k] = 0.0;
+        ph[k] = 0.0;
+        if (fs[k] < 0) continue;
+        double coeff;
+        ph[k] = prc_slot(m, a, C, r, base + (k << 5), cs[k], R, coeff);
+        if (__ldg(&m.slotFlags[base + (k << 5)]) & 1) {
+          vals[k] = -coeff;
+          pd += coeff;
+        }
+        if (r < cs[k]) {
+          div += ph[k];
+        } else {
+          div -= ph[k];
+          fs[k] = -1;
+        }
       }
-      const int c = __ldg(&m.col[e]);
-      const bool own = r < c;
-      double lam, g, t[3], d[3];
-      load_slot(m, e, lam, g, t, d);
-      const int P = own ? r : c, N = own ? c : r;
-      const double l1 = 1.0 - lam;
-      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
-      if (__ldg(&m.slotFlags[e]) & 1) {
-        const double coeff = g * rAUf;
-        a.val[e] = (M)(-coeff);
-        pd += coeff;
-      } else {
-        a.val[e] = M(0);
+      const int W = (__ldg(&m.sliceOff[(r >> 5) + 1]) - __ldg(&m.sliceOff[r >> 5])) >> 5;
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        if (k < W) a.val[base + (k << 5)] = (M)vals[k];
+        if (fs[k] >= 0) a.phiStar[fs[k]] = ph[k];
       }
-      const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
-      const double ub = l1 * U0[P] + lam * U0[N], vb = l1 * U1[P] + lam * U1[N], wb = l1 * U2[P] + lam * U2[N];
-      const double gx = l1 * Gp[P] + lam * Gp[N], gy = l1 * Gp[C + P] + lam * Gp[C + N],
-                   gz = l1 * Gp[2 * C + P] + lam * Gp[2 * C + N];
-      const double phiI = rho * (ub * S0 + vb * S1 + wb * S2);
-      const double rc = rho * g * rAUf * ((a.P[N] - a.P[P]) - (gx * d[0] + gy * d[1] + gz * d[2]));
-      const double phi = phiI - rc;
-      if (own) {
-        div += phi;
-        a.phiStar[f] = phi;
-      } else {
-        div -= phi;
+    } else {
+      int W;
+      const int base = row_base(m, r, W);
+      for (int k = 0; k < W; ++k) {
+        const int e = base + (k << 5);
+        const int f = __ldg(&m.slotFace[e]);
+        if (f < 0) {
+          a.val[e] = M(0);
+          continue;
+        }
+        const int c = __ldg(&m.col[e]);
+        double coeff;
+        const double phi = prc_slot(m, a, C, r, e, c, R, coeff);
+        if (__ldg(&m.slotFlags[e]) & 1) {
+          a.val[e] = (M)(-coeff);
+          pd += coeff;
+        } else {
+          a.val[e] = M(0);
+        }
+        if (r < c) {
+          div += phi;
+          a.phiStar[f] = phi;
+        } else {
+          div -= phi;
+        }
       }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
@@ -225,10 +350,10 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a)
       double g, t[3], S[3], d[3];
       load_bnd(m.bnd, bf, g, t, S, d);
       const unsigned ty = __ldg(&m.bType[bf]);
-      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 1)) pd += g * rAUr;
-      const double uf = (ty & 1u) ? m.bVal[bf] : U0[r];
-      const double vf = (ty & 2u) ? m.bVal[m.nBoundary + bf] : U1[r];
-      const double wf = (ty & 4u) ? m.bVal[2 * m.nBoundary + bf] : U2[r];
+      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 1)) pd += g * R.rau;
+      const double uf = (ty & 1u) ? m.bVal[bf] : R.u[0];
+      const double vf = (ty & 2u) ? m.bVal[m.nBoundary + bf] : R.u[1];
+      const double wf = (ty & 4u) ? m.bVal[2 * m.nBoundary + bf] : R.u[2];
       const double phi = rho * (uf * S[0] + vf * S[1] + wf * S[2]);
       div += phi;
       a.phiStar[nI + bf] = phi;
@@ -242,36 +367,56 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a)
 }
 
 // ---- non-orthogonal divergence (K16) + pressure rhs (K17): main.cu:1538-1604 --------------
+__device__ __forceinline__ double nonorth_slot(const DMesh& m, const NonOrthArgs& a, int C, int r, int e, int c,
+                                               double rAUr, const double (&gr)[3]) {
+  const bool own = r < c;
+  double lam, g, t[3], d[3];
+  load_slot(m, e, lam, g, t, d);
+  const double l1 = 1.0 - lam;
+  const double rc_ = __ldg(&a.rau[c]);
+  const double rAUf = l1 * (own ? rAUr : rc_) + lam * (own ? rc_ : rAUr);
+  double gf[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const double y = __ldg(&a.Gc[q * C + c]);
+    gf[q] = l1 * (own ? gr[q] : y) + lam * (own ? y : gr[q]);
+  }
+  const double flux = rAUf * (gf[0] * t[0] + gf[1] * t[1] + gf[2] * t[2]);
+  return own ? flux : -flux;
+}
+
+template <int WM>
 __global__ void __launch_bounds__(kBlock) k_nonorth_rhs(DMesh m, NonOrthArgs a) {
   const int C = m.nCells;
   const double* Gc = a.Gc;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
     double dno = 0.0;
-    int W;
-    const int base = row_base(m, r, W);
-    for (int k = 0; k < W; ++k) {
-      const int e = base + (k << 5);
-      const int f = __ldg(&m.slotFace[e]);
-      if (f < 0) break;
-      if (!(__ldg(&m.slotFlags[e]) & 2)) continue;
-      const int c = __ldg(&m.col[e]);
-      const bool own = r < c;
-      double lam, g, t[3], d[3];
-      load_slot(m, e, lam, g, t, d);
-      const int P = own ? r : c, N = own ? c : r;
-      const double l1 = 1.0 - lam;
-      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
-      const double gx = l1 * Gc[P] + lam * Gc[N], gy = l1 * Gc[C + P] + lam * Gc[C + N],
-                   gz = l1 * Gc[2 * C + P] + lam * Gc[2 * C + N];
-      const double flux = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
-      dno += own ? flux : -flux;
+    const double rAUr = __ldg(&a.rau[r]);
+    const double gr[3] = {__ldg(&Gc[r]), __ldg(&Gc[C + r]), __ldg(&Gc[2 * C + r])};
+    if constexpr (WM > 0) {
+      int fs[WM], cs[WM];
+      const int base = slot_regs<WM>(m, r, fs, cs);
+#pragma unroll
+      for (int k = 0; k < WM; ++k)
+        if (fs[k] >= 0 && (__ldg(&m.slotFlags[base + (k << 5)]) & 2))
+          dno += nonorth_slot(m, a, C, r, base + (k << 5), cs[k], rAUr, gr);
+    } else {
+      int W;
+      const int base = row_base(m, r, W);
+      for (int k = 0; k < W; ++k) {
+        const int e = base + (k << 5);
+        const int f = __ldg(&m.slotFace[e]);
+        if (f < 0) break;
+        if (!(__ldg(&m.slotFlags[e]) & 2)) continue;
+        dno += nonorth_slot(m, a, C, r, e, __ldg(&m.col[e]), rAUr, gr);
+      }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
     for (int j = j0; j < j1; ++j) {
       const int bf = __ldg(&m.cbList[j]);
       if (!(__ldg(&m.bType[bf]) & 8u) || !(__ldg(&m.bFlags[bf]) & 2)) continue;
       const double* t = m.bnd[bf].t;
-      dno += a.rau[r] * (Gc[r] * t[0] + Gc[C + r] * t[1] + Gc[2 * C + r] * t[2]);
+      dno += rAUr * (gr[0] * t[0] + gr[1] * t[1] + gr[2] * t[2]);
     }
     a.b[r] = -a.divBase[r] + dno;
   }
@@ -279,6 +424,32 @@ __global__ void __launch_bounds__(kBlock) k_nonorth_rhs(DMesh m, NonOrthArgs a) 
 
 // ---- flux correction (K16 + K19) + continuity (K15) [+ K21, K20, step statistics] ----------
 // main.cu:1615-1658, 1523-1536, 3568-3603.
+// Corrected flux of internal slot e (face f, neighbour c) of row r, in the face's owner
+// orientation: both rows of a face evaluate the same expression on the same values, so the
+// owner's phi and the neighbour's are equal bit for bit.  Row values (rAU, p', grad p') come in
+// registers; all loads are read-only.
+__device__ __forceinline__ double flux_slot(const DMesh& m, const FluxArgs& a, int C, int r, int e, int f, int c,
+                                            double rAUr, double pcr, const double (&gr)[3], bool& own) {
+  own = r < c;
+  double lam, g, t[3], d[3];
+  load_slot(m, e, lam, g, t, d);
+  const double rAUc = __ldg(&a.rau[c]), pcc = __ldg(&a.pc[c]);
+  const double rP = own ? rAUr : rAUc, rN = own ? rAUc : rAUr;
+  const double pP = own ? pcr : pcc, pN = own ? pcc : pcr;
+  const double l1 = 1.0 - lam;
+  const double rAUf = l1 * rP + lam * rN;
+  double phiNO = 0.0;
+  if (__ldg(&m.slotFlags[e]) & 2) {
+    const double c0 = __ldg(&a.Gc[c]), c1 = __ldg(&a.Gc[C + c]), c2 = __ldg(&a.Gc[2 * C + c]);
+    const double gx = l1 * (own ? gr[0] : c0) + lam * (own ? c0 : gr[0]);
+    const double gy = l1 * (own ? gr[1] : c1) + lam * (own ? c1 : gr[1]);
+    const double gz = l1 * (own ? gr[2] : c2) + lam * (own ? c2 : gr[2]);
+    phiNO = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
+  }
+  return __ldg(&a.phiStar[f]) - g * rAUf * (pN - pP) - phiNO;
+}
+
+template <int WM>
 __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
   __shared__ double sm[9 * 32];
   const int C = m.nCells, nI = m.nInternal;
@@ -286,32 +457,44 @@ __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
     double div = 0.0;
-    const double pcr = a.pc[r], rAUr = a.rau[r];
-    int W;
-    const int base = row_base(m, r, W);
-    for (int k = 0; k < W; ++k) {
-      const int e = base + (k << 5);
-      const int f = __ldg(&m.slotFace[e]);
-      if (f < 0) break;
-      const int c = __ldg(&m.col[e]);
-      const bool own = r < c;
-      double lam, g, t[3], d[3];
-      load_slot(m, e, lam, g, t, d);
-      const int P = own ? r : c, N = own ? c : r;
-      const double l1 = 1.0 - lam;
-      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
-      double phiNO = 0.0;
-      if (__ldg(&m.slotFlags[e]) & 2) {
-        const double gx = l1 * Gc[P] + lam * Gc[N], gy = l1 * Gc[C + P] + lam * Gc[C + N],
-                     gz = l1 * Gc[2 * C + P] + lam * Gc[2 * C + N];
-        phiNO = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
+    const double pcr = __ldg(&a.pc[r]), rAUr = __ldg(&a.rau[r]);
+    const double gr[3] = {__ldg(&Gc[r]), __ldg(&Gc[C + r]), __ldg(&Gc[2 * C + r])};
+    if constexpr (WM > 0) {
+      // every load of the row first, the owner's flux stores after the loop
+      int fs[WM], cs[WM];
+      const int base = slot_regs<WM>(m, r, fs, cs);
+      double ph[WM];
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        ph[k] = 0.0;
+        if (fs[k] < 0) continue;
+        bool own;
+        ph[k] = flux_slot(m, a, C, r, base + (k << 5), fs[k], cs[k], rAUr, pcr, gr, own);
+        if (own) {
+          div += ph[k];
+        } else {
+          div -= ph[k];
+          fs[k] = -1;
+        }
       }
-      const double phi = a.phiStar[f] - g * rAUf * (a.pc[N] - a.pc[P]) - phiNO;
-      if (own) {
-        div += phi;
-        a.phi[f] = phi;
-      } else {
-        div -= phi;
+#pragma unroll
+      for (int k = 0; k < WM; ++k)
+        if (fs[k] >= 0) a.phi[fs[k]] = ph[k];
+    } else {
+      int W;
+      const int base = row_base(m, r, W);
+      for (int k = 0; k < W; ++k) {
+        const int e = base + (k << 5);
+        const int f = __ldg(&m.slotFace[e]);
+        if (f < 0) break;
+        bool own;
+        const double phi = flux_slot(m, a, C, r, e, f, __ldg(&m.col[e]), rAUr, pcr, gr, own);
+        if (own) {
+          div += phi;
+          a.phi[f] = phi;
+        } else {
+          div -= phi;
+        }
       }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
@@ -322,7 +505,7 @@ __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
       if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 2)) {
         const double g = m.bnd[bf].g;
         const double* t = m.bnd[bf].t;
-        const double phiNO = rAUr * (Gc[r] * t[0] + Gc[C + r] * t[1] + Gc[2 * C + r] * t[2]);
+        const double phiNO = rAUr * (gr[0] * t[0] + gr[1] * t[1] + gr[2] * t[2]);
         phi = phi - g * rAUr * (m.bVal[3 * m.nBoundary + bf] - pcr) - phiNO;
       }
       div += phi;
@@ -336,7 +519,7 @@ __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const double uo = a.U[q * C + r];
-        const double un = a.Us[q * C + r] - rAUr * Gc[q * C + r];
+        const double un = a.Us[q * C + r] - rAUr * gr[q];
         a.U[q * C + r] = un;
         const double dd = un - uo;
         acc[2 * q] += dd * dd;
@@ -433,22 +616,35 @@ double AlgoBytes::flux_final() const {
 double AlgoBytes::bicg_spmv(int nc) const { return 8.0 * C + 12.0 * nnzOff + 24.0 * nc * C; }
 double AlgoBytes::pcg_spmv() const { return 40.0 * C + 12.0 * nnzOff; }
 
+template <int WM>
+static void lsq_grad_w(const LaunchCfg& lc, const DMesh& m, const GradArgs& a) {
+  if (a.nf == 4) k_lsq_grad<4, WM><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (a.nf == 3) k_lsq_grad<3, WM><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (a.nf == 2) k_lsq_grad<2, WM><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else k_lsq_grad<1, WM><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+}
 void launch_lsq_grad(const LaunchCfg& lc, const DMesh& m, const GradArgs& a) {
   ProfScope ps(lc, kKfGradient, lc.ab ? lc.ab->gradient(a.nf) : 0.0);
-  if (a.nf == 4) k_lsq_grad<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
-  else if (a.nf == 3) k_lsq_grad<3><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
-  else if (a.nf == 2) k_lsq_grad<2><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
-  else k_lsq_grad<1><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  const int wc = sell_width_class(m.maxW);
+  if (wc == 4) lsq_grad_w<4>(lc, m, a);
+  else if (wc == 8) lsq_grad_w<8>(lc, m, a);
+  else lsq_grad_w<0>(lc, m, a);
 }
 template <class M>
 void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgsT<M>& a) {
   ProfScope ps(lc, kKfMomentum, lc.ab ? lc.ab->momentum() : 0.0);
-  k_momentum<M><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  const int wc = sell_width_class(m.maxW);
+  if (wc == 4) k_momentum<M, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 8) k_momentum<M, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else k_momentum<M, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 template <class M>
 void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgsT<M>& a) {
   ProfScope ps(lc, kKfPressureRc, lc.ab ? lc.ab->pressure_rc() : 0.0);
-  k_pressure_rc<M><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  const int wc = sell_width_class(m.maxW);
+  if (wc == 4) k_pressure_rc<M, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 8) k_pressure_rc<M, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else k_pressure_rc<M, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 template void launch_momentum<double>(const LaunchCfg&, const DMesh&, const MomArgsT<double>&);
 template void launch_momentum<float>(const LaunchCfg&, const DMesh&, const MomArgsT<float>&);
@@ -456,11 +652,17 @@ template void launch_pressure_rc<double>(const LaunchCfg&, const DMesh&, const P
 template void launch_pressure_rc<float>(const LaunchCfg&, const DMesh&, const PresArgsT<float>&);
 void launch_nonorth_rhs(const LaunchCfg& lc, const DMesh& m, const NonOrthArgs& a) {
   ProfScope ps(lc, kKfNonOrth, lc.ab ? lc.ab->nonorth() : 0.0);
-  k_nonorth_rhs<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  const int wc = sell_width_class(m.maxW);
+  if (wc == 4) k_nonorth_rhs<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 8) k_nonorth_rhs<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else k_nonorth_rhs<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a) {
   ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0);
-  k_flux_final<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  const int wc = sell_width_class(m.maxW);
+  if (wc == 4) k_flux_final<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 8) k_flux_final<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else k_flux_final<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_patch_force(cudaStream_t s, const DMesh& m, int b0, int b1, int sign, double mu, const double* bA,
                         const double* bN, const double* U, const double* P, double* out) {
