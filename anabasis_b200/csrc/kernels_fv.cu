@@ -147,7 +147,7 @@ __device__ __forceinline__ void momentum_slot(const DMesh& m, const MomArgsT<M>&
 }
 
 template <class M, int WM>
-__global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
+__global__ void __launch_bounds__(kBlock, 3) k_momentum(DMesh m, MomArgsT<M> a) {
   const int C = m.nCells;
   const bool full = !a.rhsOnly;
   const double* G = a.G;
@@ -241,107 +241,54 @@ __global__ void __launch_bounds__(kBlock) k_momentum(DMesh m, MomArgsT<M> a) {
 }
 
 // ---- pressure matrix (K11,K12) + Rhie-Chow flux (K14) + continuity (K15) ------------------
-// main.cu:1898-1950, 1474-1536, launch sequence 3407-3452.
-// Internal slot e (neighbour c) of row r: the pressure coefficient g rAU_f (returned through
-// coeff) and the Rhie-Chow flux in owner orientation, equal bit for bit from both sides.  Row
-// values come in registers.
-struct PresRow {
-  double rau, u[3], gp[3], p;
-};
+// main.cu:1898-1950, 1474-1536, launch sequence 3407-3452.  The plain slot loop measured faster
+// here than the register-staged form of the other face kernels (many gathers per slot).
 template <class M>
-__device__ __forceinline__ double prc_slot(const DMesh& m, const PresArgsT<M>& a, int C, int r, int e, int c,
-                                           const PresRow& R, double& coeff) {
-  const bool own = r < c;
-  double lam, g, t[3], d[3];
-  load_slot(m, e, lam, g, t, d);
-  const double l1 = 1.0 - lam;
-  const double rc_ = __ldg(&a.rau[c]);
-  const double rAUf = l1 * (own ? R.rau : rc_) + lam * (own ? rc_ : R.rau);
-  coeff = g * rAUf;
-  const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
-  double uf[3], gf[3];
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    const double x = __ldg(&a.Us[q * C + c]);
-    uf[q] = l1 * (own ? R.u[q] : x) + lam * (own ? x : R.u[q]);
-    const double y = __ldg(&a.Gp[q * C + c]);
-    gf[q] = l1 * (own ? R.gp[q] : y) + lam * (own ? y : R.gp[q]);
-  }
-  const double pc_ = __ldg(&a.P[c]);
-  const double pP = own ? R.p : pc_, pN = own ? pc_ : R.p;
-  const double phiI = a.rho * (uf[0] * S0 + uf[1] * S1 + uf[2] * S2);
-  const double rc = a.rho * g * rAUf * ((pN - pP) - (gf[0] * d[0] + gf[1] * d[1] + gf[2] * d[2]));
-  return phiI - rc;
-}
-
-template <class M, int WM>
 __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a) {
   const int C = m.nCells, nI = m.nInternal;
+  const double* U0 = a.Us;
+  const double* U1 = a.Us + C;
+  const double* U2 = a.Us + 2 * C;
+  const double* Gp = a.Gp;
   const double rho = a.rho;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
     double pd = 0.0, div = 0.0;
-    PresRow R;
-    R.rau = __ldg(&a.rau[r]);
-    R.p = __ldg(&a.P[r]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      R.u[q] = __ldg(&a.Us[q * C + r]);
-      R.gp[q] = __ldg(&a.Gp[q * C + r]);
-    }
-    if constexpr (WM > 0) {
-      // every load of the row first, the stores after the loop
-      int fs[WM], cs[WM];
-      const int base = slot_regs<WM>(m, r, fs, cs);
-      double vals[WM], ph[WM];
-#pragma unroll
-      for (int k = 0; k < WM; ++k) {
-        vals[k] = 0.0;
-        ph[k] = 0.0;
-        if (fs[k] < 0) continue;
-        double coeff;
-        ph[k] = prc_slot(m, a, C, r, base + (k << 5), cs[k], R, coeff);
-        if (__ldg(&m.slotFlags[base + (k << 5)]) & 1) {
-          vals[k] = -coeff;
-          pd += coeff;
-        }
-        if (r < cs[k]) {
-          div += ph[k];
-        } else {
-          div -= ph[k];
-          fs[k] = -1;
-        }
+    const double rAUr = a.rau[r];
+    int W;
+    const int base = row_base(m, r, W);
+    for (int k = 0; k < W; ++k) {
+      const int e = base + (k << 5);
+      const int f = __ldg(&m.slotFace[e]);
+      if (f < 0) {
+        a.val[e] = M(0);
+        continue;
       }
-      const int W = (__ldg(&m.sliceOff[(r >> 5) + 1]) - __ldg(&m.sliceOff[r >> 5])) >> 5;
-#pragma unroll
-      for (int k = 0; k < WM; ++k) {
-        if (k < W) a.val[base + (k << 5)] = (M)vals[k];
-        if (fs[k] >= 0) a.phiStar[fs[k]] = ph[k];
+      const int c = __ldg(&m.col[e]);
+      const bool own = r < c;
+      double lam, g, t[3], d[3];
+      load_slot(m, e, lam, g, t, d);
+      const int P = own ? r : c, N = own ? c : r;
+      const double l1 = 1.0 - lam;
+      const double rAUf = l1 * a.rau[P] + lam * a.rau[N];
+      if (__ldg(&m.slotFlags[e]) & 1) {
+        const double coeff = g * rAUf;
+        a.val[e] = (M)(-coeff);
+        pd += coeff;
+      } else {
+        a.val[e] = M(0);
       }
-    } else {
-      int W;
-      const int base = row_base(m, r, W);
-      for (int k = 0; k < W; ++k) {
-        const int e = base + (k << 5);
-        const int f = __ldg(&m.slotFace[e]);
-        if (f < 0) {
-          a.val[e] = M(0);
-          continue;
-        }
-        const int c = __ldg(&m.col[e]);
-        double coeff;
-        const double phi = prc_slot(m, a, C, r, e, c, R, coeff);
-        if (__ldg(&m.slotFlags[e]) & 1) {
-          a.val[e] = (M)(-coeff);
-          pd += coeff;
-        } else {
-          a.val[e] = M(0);
-        }
-        if (r < c) {
-          div += phi;
-          a.phiStar[f] = phi;
-        } else {
-          div -= phi;
-        }
+      const double S0 = t[0] + g * d[0], S1 = t[1] + g * d[1], S2 = t[2] + g * d[2];
+      const double ub = l1 * U0[P] + lam * U0[N], vb = l1 * U1[P] + lam * U1[N], wb = l1 * U2[P] + lam * U2[N];
+      const double gx = l1 * Gp[P] + lam * Gp[N], gy = l1 * Gp[C + P] + lam * Gp[C + N],
+                   gz = l1 * Gp[2 * C + P] + lam * Gp[2 * C + N];
+      const double phiI = rho * (ub * S0 + vb * S1 + wb * S2);
+      const double rc = rho * g * rAUf * ((a.P[N] - a.P[P]) - (gx * d[0] + gy * d[1] + gz * d[2]));
+      const double phi = phiI - rc;
+      if (own) {
+        div += phi;
+        a.phiStar[f] = phi;
+      } else {
+        div -= phi;
       }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
@@ -350,10 +297,10 @@ __global__ void __launch_bounds__(kBlock) k_pressure_rc(DMesh m, PresArgsT<M> a)
       double g, t[3], S[3], d[3];
       load_bnd(m.bnd, bf, g, t, S, d);
       const unsigned ty = __ldg(&m.bType[bf]);
-      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 1)) pd += g * R.rau;
-      const double uf = (ty & 1u) ? m.bVal[bf] : R.u[0];
-      const double vf = (ty & 2u) ? m.bVal[m.nBoundary + bf] : R.u[1];
-      const double wf = (ty & 4u) ? m.bVal[2 * m.nBoundary + bf] : R.u[2];
+      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 1)) pd += g * rAUr;
+      const double uf = (ty & 1u) ? m.bVal[bf] : U0[r];
+      const double vf = (ty & 2u) ? m.bVal[m.nBoundary + bf] : U1[r];
+      const double wf = (ty & 4u) ? m.bVal[2 * m.nBoundary + bf] : U2[r];
       const double phi = rho * (uf * S[0] + vf * S[1] + wf * S[2]);
       div += phi;
       a.phiStar[nI + bf] = phi;
@@ -386,7 +333,7 @@ __device__ __forceinline__ double nonorth_slot(const DMesh& m, const NonOrthArgs
 }
 
 template <int WM>
-__global__ void __launch_bounds__(kBlock) k_nonorth_rhs(DMesh m, NonOrthArgs a) {
+__global__ void __launch_bounds__(kBlock, 6) k_nonorth_rhs(DMesh m, NonOrthArgs a) {
   const int C = m.nCells;
   const double* Gc = a.Gc;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
@@ -641,10 +588,7 @@ void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgsT<M>& a) 
 template <class M>
 void launch_pressure_rc(const LaunchCfg& lc, const DMesh& m, const PresArgsT<M>& a) {
   ProfScope ps(lc, kKfPressureRc, lc.ab ? lc.ab->pressure_rc() : 0.0);
-  const int wc = sell_width_class(m.maxW);
-  if (wc == 4) k_pressure_rc<M, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
-  else if (wc == 8) k_pressure_rc<M, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
-  else k_pressure_rc<M, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  k_pressure_rc<M><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 template void launch_momentum<double>(const LaunchCfg&, const DMesh&, const MomArgsT<double>&);
 template void launch_momentum<float>(const LaunchCfg&, const DMesh&, const MomArgsT<float>&);
