@@ -156,12 +156,15 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
     for (int i = 0; i < A.n; ++i) agg[i] = i;
     int nc = A.n;
     HCsr B = A;
-    for (int pass = 0; pass < opt.passesPerLevel; ++pass) {
+    const size_t lev = levels.size() - 1;
+    const int nPass = opt.passes.empty() ? opt.passesPerLevel
+                                         : opt.passes[std::min(lev, opt.passes.size() - 1)];
+    for (int pass = 0; pass < nPass; ++pass) {
       int ncp = 0;
       std::vector<int> a = pairwise(B, opt.strength, ncp);
       for (int i = 0; i < A.n; ++i) agg[i] = a[agg[i]];
       nc = ncp;
-      if (pass + 1 < opt.passesPerLevel) B = galerkin(B, a, ncp);
+      if (pass + 1 < nPass) B = galerkin(B, a, ncp);
     }
     if (nc > (int)(0.9 * A.n) || nc < 1) break;  // coarsening stalled
     HCsr Cc = galerkin(A, agg, nc);

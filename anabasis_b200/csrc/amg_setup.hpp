@@ -38,6 +38,9 @@ struct AmgSetupOptions {
   int coarseMax = 128;   // dense solve at or below this size
   int maxLevels = 24;
   int passesPerLevel = 2;
+  // pairwise passes for the coarsening of level l (l = 0, 1, ...); the last entry repeats, and an
+  // empty list means passesPerLevel everywhere
+  std::vector<int> passes;
 };
 
 // vals / diag are the level-0 matrix in the layout's SELL-32 storage.

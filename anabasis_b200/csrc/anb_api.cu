@@ -234,6 +234,10 @@ PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, do
 // 0 launches every level and sweep separately).  The arithmetic is the same either way.
 constexpr int kAmgTailRows = 1024;
 
+// Grid of the row-parallel kernels: at most this many 256-thread blocks per SM (grid-stride
+// beyond); ANB_BLOCKS_PER_SM overrides.
+constexpr int kBlocksPerSM = 8;
+
 // Aggregation hierarchy for the current level-0 matrix (val0/diag0 on the device, storage type T),
 // coarse levels in T, coarsest inverse in double; the V-cycle is captured as a graph for `ga`.
 template <class T>
@@ -243,6 +247,13 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
   CK(cudaMemcpyAsync(hd.data(), diag0, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   AmgSetupOptions opt;
+  if (const char* ps = std::getenv("ANB_AMG_PASSES")) {  // e.g. "2,2,3": passes per level
+    for (const char* q = ps; *q;) {
+      opt.passes.push_back(std::max(1, std::atoi(q)));
+      while (*q && *q != ',') ++q;
+      if (*q == ',') ++q;
+    }
+  }
   c->amgHost = build_amg_hierarchy(c->L, std::vector<double>(hv.begin(), hv.end()),
                                    std::vector<double>(hd.begin(), hd.end()), opt);
   A.nLevels = (int)c->amgHost.size();
@@ -777,7 +788,11 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     int nSM = 148;
     CK(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, prm->device));
     c->lc.stream = c->stream;
-    c->lc.rowBlocks = std::max(1, std::min((c->C + kBlock - 1) / kBlock, nSM * 8));
+    {
+      const char* bps = std::getenv("ANB_BLOCKS_PER_SM");
+      const int perSM = bps ? std::max(1, std::min(64, std::atoi(bps))) : kBlocksPerSM;
+      c->lc.rowBlocks = std::max(1, std::min((c->C + kBlock - 1) / kBlock, nSM * perSM));
+    }
     c->lc.prof = &c->prof;
     c->lc.ab = &c->ab;
     c->ab.C = c->C;
@@ -910,7 +925,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     c->flags = A.alloc<int>(32);
     c->stats = A.alloc<double>(16);
     c->forceOut = A.alloc<double>(16);
-    c->red.partials = A.alloc<double>((size_t)(nSM * 8 + 16) * 16);
+    c->red.partials = A.alloc<double>((size_t)(c->lc.rowBlocks + 16) * 16);
     c->red.ticket = A.alloc<unsigned int>(1);
     CK(cudaMemset(c->red.ticket, 0, sizeof(unsigned int)));
     if (!c->mixed) {
