@@ -715,6 +715,8 @@ __global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDevT<T> f, T* v
 // Dense inverse of the coarsest matrix by in-place Gauss-Jordan in double (SPD, no pivoting
 // needed); a pivot below 1e-13 of the largest diagonal (singular, all-Neumann systems) gets a
 // zero row/column, i.e. the correction ignores the null direction.  One block, shared memory.
+constexpr int kDenseMax = 160;  // largest coarsest level (rows)
+
 template <class T>
 __global__ void k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
   extern __shared__ double A[];
@@ -736,15 +738,16 @@ __global__ void k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
     dmax = mx;
   }
   __syncthreads();
-  __shared__ double piv;
-  __shared__ int skip;
+  // Each pivot step in two phases: (a) the scaled pivot row and the old pivot column are copied
+  // out, (b) every entry is updated from the copies, so a step needs two barriers and no entry is
+  // read after another thread changed it.  The arithmetic per entry is the textbook step:
+  // row k / piv, A_kk = 1 / piv, A_ij -= A_ik (A_kj / piv), A_ik = -A_ik / piv.
+  __shared__ double rowk[kDenseMax], colk[kDenseMax];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int k = 0; k < n; ++k) {
-    if (threadIdx.x == 0) {
-      piv = A[k * n + k];
-      skip = fabs(piv) <= 1e-13 * dmax;
-    }
-    __syncthreads();
-    if (skip) {
+    const double piv = A[k * n + k];  // read by every thread: the same value, so one branch
+    if (fabs(piv) <= 1e-13 * dmax) {
+      __syncthreads();
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
         A[k * n + j] = 0.0;
         A[j * n + k] = 0.0;
@@ -752,19 +755,20 @@ __global__ void k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
       __syncthreads();
       continue;
     }
-    for (int j = threadIdx.x; j < n; j += blockDim.x)
-      if (j != k) A[k * n + j] /= piv;
-    __syncthreads();
-    if (threadIdx.x == 0) A[k * n + k] = 1.0 / piv;
-    __syncthreads();
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-      const int i = t / n, j = t % n;
-      if (i == k || j == k) continue;
-      A[t] -= A[i * n + k] * A[k * n + j];
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      rowk[j] = j == k ? 1.0 / piv : A[k * n + j] / piv;
+      colk[j] = A[j * n + k];
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x)
-      if (i != k) A[i * n + k] = -A[i * n + k] * A[k * n + k];
+    for (int i = wid; i < n; i += nw) {
+      const double cik = colk[i];
+      for (int j = lane; j < n; j += 32) {
+        double& a = A[i * n + j];
+        if (i == k) a = rowk[j];
+        else if (j == k) a = -cik * rowk[k];
+        else a -= cik * rowk[j];
+      }
+    }
     __syncthreads();
   }
   for (int t = threadIdx.x; t < n * n; t += blockDim.x) inv[t] = A[t];
