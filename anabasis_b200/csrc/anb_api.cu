@@ -233,6 +233,9 @@ PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, do
 // Coarse levels of at most this many rows run as one cluster kernel (ANB_AMG_TAIL_ROWS overrides;
 // 0 launches every level and sweep separately).  The arithmetic is the same either way.
 constexpr int kAmgTailRows = 1024;
+// CSR levels of at most this many rows run down sweep + restriction as one kernel
+// (ANB_AMG_FUSED_DOWN_ROWS overrides; 0 = off).  Same values either way.
+constexpr int kAmgFusedDownRows = 65536;
 
 // Grid of the row-parallel kernels: at most this many 256-thread blocks per SM (grid-stride
 // beyond); ANB_BLOCKS_PER_SM overrides.
@@ -297,6 +300,8 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
   c->amgBuilt = true;
   const char* tailEnv = std::getenv("ANB_AMG_TAIL_ROWS");
   amg_configure_tail(A, tailEnv ? std::atoi(tailEnv) : kAmgTailRows, c->stream);
+  const char* fdEnv = std::getenv("ANB_AMG_FUSED_DOWN_ROWS");
+  A.fusedDownRows = fdEnv ? std::atoi(fdEnv) : kAmgFusedDownRows;
   const char* verbose = std::getenv("ANB_AMG_VERBOSE");
   if (verbose && verbose[0] == '1') {
     std::fprintf(stderr, "AMG levels:");

@@ -275,6 +275,9 @@ struct AmgDevT {
   // thread-block-cluster kernel of tailCluster CTAs (0: one launch per level and sweep).
   int tailRows = 0;
   int tailCluster = 0;
+  // CSR levels of at most this many rows (above the tail) run their down sweep and restriction
+  // as one kernel, warp per aggregate (same values; fewer launches, longer chains per warp)
+  int fusedDownRows = 0;
 };
 using AmgLevelDev = AmgLevelDevT<double>;
 using AmgDev = AmgDevT<double>;

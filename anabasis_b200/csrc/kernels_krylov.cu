@@ -530,6 +530,49 @@ __device__ __forceinline__ void resid_csr_rows(const AmgLevelDevT<T>& f, int war
   }
 }
 
+// Down on a CSR level in one sweep: warp per aggregate I of the next level, its member rows G
+// lanes each (32/G at a time); x = w D^-1 b for every member and b_next[I] = the sum over the
+// members, in member order, of their T-rounded residuals b - A x.  These are the values of
+// resid_csr_rows followed by restrict_rows without the round trip of r through memory and with
+// one launch instead of two; an aggregate's members run one after another, so the sweep pays off
+// on the small levels only (kFusedDownRows).
+template <int G, class T, class LD>
+__device__ __forceinline__ void down_csr_aggs(const AmgLevelDevT<T>& f, T* bNext, int warp, int nWarps, LD ldv) {
+  const int lane = threadIdx.x & 31, sub = lane % G, grp = lane / G;
+  constexpr int NG = 32 / G;
+  for (int I = warp; I < f.nc; I += nWarps) {
+    const int m0 = __ldg(&f.memOff[I]), m1 = __ldg(&f.memOff[I + 1]);
+    double sum = 0.0;
+    for (int mb = m0; mb < m1; mb += NG) {
+      const int mm = mb + grp;
+      double acc = 0.0;
+      int i = 0;
+      if (mm < m1) {
+        i = __ldg(&f.mem[mm]);
+        const int k1 = __ldg(&f.rowOff[i + 1]);
+        for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
+          const int j = __ldg(&f.col[k]);
+          acc += ld(&f.val[k]) * (ld(&f.wdinv[j]) * ldv(&f.b[j]));
+        }
+      }
+      acc = group_sum<G>(acc);
+      double r = 0.0;
+      if (mm < m1 && sub == 0) {
+        const double di = ld(&f.diag[i]), bi = ldv(&f.b[i]);
+        const double xi = ld(&f.wdinv[i]) * bi;
+        f.x[i] = (T)xi;
+        r = (double)(T)(bi - di * xi - acc);
+      }
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        const double rg = __shfl_sync(0xffffffffu, r, g * G);
+        if (mb + g < m1) sum += rg;
+      }
+    }
+    if (lane == 0) bNext[I] = (T)sum;
+  }
+}
+
 // Up on a CSR level: out = xt + w D^-1 (b - A xt) with xt = x + corr e[agg].
 template <int G, class T, class LD>
 __device__ __forceinline__ void up_csr_rows(const AmgLevelDevT<T>& f, const T* e, double corr, T* out, int warp,
@@ -585,6 +628,12 @@ template <int G, class T>
 __global__ void __launch_bounds__(kBlock) k_amg_resid_csr(const int* done, AmgLevelDevT<T> f, double omega) {
   if (*done) return;
   resid_csr_rows<G>(f, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, (gridDim.x * blockDim.x) >> 5, LdRO{});
+}
+
+template <int G, class T>
+__global__ void __launch_bounds__(kBlock) k_amg_down_csr(const int* done, AmgLevelDevT<T> f, T* bNext) {
+  if (*done) return;
+  down_csr_aggs<G>(f, bNext, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, (gridDim.x * blockDim.x) >> 5, LdRO{});
 }
 
 template <int G, class T>
@@ -932,9 +981,16 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
   }
   {
     const int t0 = tail_start(amg);
-    ProfScope ps(lc, kKfAmgCoarse, 0.0, 3 * (t0 - 1) + 1);
+    int nl = 1;
+    for (int l = 1; l < t0; ++l) nl += 2 + (amg->lv[l].n > amg->fusedDownRows ? 1 : 0);
+    ProfScope ps(lc, kKfAmgCoarse, 0.0, nl);
     for (int l = 1; l < t0; ++l) {
       const AmgLevelDevT<T>& f = amg->lv[l];
+      if (f.n <= amg->fusedDownRows) {
+        k_amg_down_csr<kCoarseLanes, T><<<blocks_for(f.nc * 32, lc.rowBlocks), kBlock, 0, lc.stream>>>(
+            a.fl, f, amg->lv[l + 1].b);
+        continue;
+      }
       k_amg_resid_csr<kCoarseLanes, T><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, amg->omega);
       k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
