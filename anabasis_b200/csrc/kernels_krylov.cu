@@ -763,12 +763,21 @@ __global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDevT<T> f, T* v
 
 // Dense inverse of the coarsest matrix by in-place Gauss-Jordan in double (SPD, no pivoting
 // needed); a pivot below 1e-13 of the largest diagonal (singular, all-Neumann systems) gets a
-// zero row/column, i.e. the correction ignores the null direction.  One block, shared memory.
+// zero row/column, i.e. the correction ignores the null direction.  One block of 32 warps: the
+// matrix is assembled in shared memory, then held in registers, warp w owning rows w, w+32, ...
+// and lane l columns l, l+32, ... (NC chunks each, n <= 32 NC).  A pivot step is one barrier:
+// the warp owning row k broadcasts the pivot by shuffle and publishes the scaled row, the lanes
+// owning column k publish the old column (double-buffered), and every thread updates its entries.
+// Per entry the arithmetic is the textbook step: row k / piv, A_kk = 1 / piv,
+// A_ij -= A_ik (A_kj / piv), A_ik = -A_ik / piv.
 constexpr int kDenseMax = 160;  // largest coarsest level (rows)
 
-template <class T>
-__global__ void k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
+template <class T, int NC>
+__global__ void __launch_bounds__(1024, 1) k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
   extern __shared__ double A[];
+  __shared__ double rowk[2][kDenseMax], colk[2][kDenseMax];
+  __shared__ int skipk[2];
+  __shared__ double dmax;
   const int n = c.n;
   for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = 0.0;
   __syncthreads();
@@ -780,47 +789,86 @@ __global__ void k_amg_dense_factor(AmgLevelDevT<T> c, double* inv) {
     }
   }
   __syncthreads();
-  __shared__ double dmax;
   if (threadIdx.x == 0) {
     double mx = 0.0;
     for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(A[i * n + i]));
     dmax = mx;
   }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double a[NC][NC];
+#pragma unroll
+  for (int p = 0; p < NC; ++p)
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const int i = w + 32 * p, j = lane + 32 * q;
+      a[p][q] = (i < n && j < n) ? A[i * n + j] : 0.0;
+    }
   __syncthreads();
-  // Each pivot step in two phases: (a) the scaled pivot row and the old pivot column are copied
-  // out, (b) every entry is updated from the copies, so a step needs two barriers and no entry is
-  // read after another thread changed it.  The arithmetic per entry is the textbook step:
-  // row k / piv, A_kk = 1 / piv, A_ij -= A_ik (A_kj / piv), A_ik = -A_ik / piv.
-  __shared__ double rowk[kDenseMax], colk[kDenseMax];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k = 0; k < n; ++k) {
-    const double piv = A[k * n + k];  // read by every thread: the same value, so one branch
-    if (fabs(piv) <= 1e-13 * dmax) {
-      __syncthreads();
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        A[k * n + j] = 0.0;
-        A[j * n + k] = 0.0;
+  const double dm = dmax;
+  // pivot k = 32 kc + kw: the chunk kc is a compile-time index, so every register access is static
+#pragma unroll
+  for (int kc = 0; kc < NC; ++kc) {
+    for (int kw = 0; kw < 32; ++kw) {
+      const int k = 32 * kc + kw;
+      if (k >= n) break;  // uniform over the block
+      const int buf = k & 1;
+      if (w == kw) {  // row k: pivot by shuffle from lane kw, scaled row to shared memory
+        const double piv = __shfl_sync(0xffffffffu, a[kc][kc], kw);
+        if (lane == 0) skipk[buf] = fabs(piv) <= 1e-13 * dm;
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          const int j = lane + 32 * q;
+          if (j < n) rowk[buf][j] = j == k ? 1.0 / piv : a[kc][q] / piv;
+        }
+      }
+      if (lane == kw) {  // column k before the step
+#pragma unroll
+        for (int p = 0; p < NC; ++p) {
+          const int i = w + 32 * p;
+          if (i < n) colk[buf][i] = a[p][kc];
+        }
       }
       __syncthreads();
-      continue;
-    }
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-      rowk[j] = j == k ? 1.0 / piv : A[k * n + j] / piv;
-      colk[j] = A[j * n + k];
-    }
-    __syncthreads();
-    for (int i = wid; i < n; i += nw) {
-      const double cik = colk[i];
-      for (int j = lane; j < n; j += 32) {
-        double& a = A[i * n + j];
-        if (i == k) a = rowk[j];
-        else if (j == k) a = -cik * rowk[k];
-        else a -= cik * rowk[j];
+      // every entry takes the rank-1 update, then column k and row k (in that order) are
+      // overwritten by their owners; entries past n stay zero and are never stored
+      if (skipk[buf] == 0) {
+        double rk[NC], ck[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) rk[q] = lane + 32 * q < n ? rowk[buf][lane + 32 * q] : 0.0;
+#pragma unroll
+        for (int p = 0; p < NC; ++p) ck[p] = w + 32 * p < n ? colk[buf][w + 32 * p] : 0.0;
+#pragma unroll
+        for (int p = 0; p < NC; ++p)
+#pragma unroll
+          for (int q = 0; q < NC; ++q) a[p][q] -= ck[p] * rk[q];
+        if (lane == kw) {
+          const double rkk = rowk[buf][k];
+#pragma unroll
+          for (int p = 0; p < NC; ++p) a[p][kc] = -ck[p] * rkk;
+        }
+        if (w == kw) {
+#pragma unroll
+          for (int q = 0; q < NC; ++q) a[kc][q] = rk[q];
+        }
+      } else {
+        if (lane == kw) {
+#pragma unroll
+          for (int p = 0; p < NC; ++p) a[p][kc] = 0.0;
+        }
+        if (w == kw) {
+#pragma unroll
+          for (int q = 0; q < NC; ++q) a[kc][q] = 0.0;
+        }
       }
     }
-    __syncthreads();
   }
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) inv[t] = A[t];
+#pragma unroll
+  for (int p = 0; p < NC; ++p)
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const int i = w + 32 * p, j = lane + 32 * q;
+      if (i < n && j < n) inv[(size_t)i * n + j] = a[p][q];
+    }
 }
 
 // ---------------------------------------------------------------- mixed-precision defect
@@ -1091,9 +1139,17 @@ void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg) {
   }
   const AmgLevelDevT<T>& c = amg.lv[amg.nLevels - 1];
   const size_t smem = sizeof(double) * (size_t)c.n * c.n;
-  cudaFuncSetAttribute(k_amg_dense_factor<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   g_launches += 1;
-  k_amg_dense_factor<T><<<1, 1024, smem, lc.stream>>>(c, amg.dense);
+  const int nc = (c.n + 31) / 32;
+  auto go = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    kern<<<1, 1024, smem, lc.stream>>>(c, amg.dense);
+  };
+  if (nc <= 1) go(k_amg_dense_factor<T, 1>);
+  else if (nc == 2) go(k_amg_dense_factor<T, 2>);
+  else if (nc == 3) go(k_amg_dense_factor<T, 3>);
+  else if (nc == 4) go(k_amg_dense_factor<T, 4>);
+  else go(k_amg_dense_factor<T, 5>);
 }
 
 void launch_defect(const LaunchCfg& lc, const DefectArgs& a) {
