@@ -52,12 +52,14 @@ __device__ __forceinline__ void sell_row3(const DSellT<T>& A, int r, const T* x,
   const int b = __ldg(&A.sliceOff[s]) + (r & 31);
   const int W = (__ldg(&A.sliceOff[s + 1]) - __ldg(&A.sliceOff[s])) >> 5;
   const double d = (double)A.diag[r];
+#pragma unroll
   for (int c = 0; c < 3; ++c) y[c] = (c < nc && act[c]) ? d * (double)x[c * n + r] : 0.0;
 #pragma unroll 2
   for (int k = 0; k < W; ++k) {
     const int e = b + (k << 5);
     const double v = ld(&A.val[e]);
     const int j = __ldg(&A.col[e]);
+#pragma unroll
     for (int c = 0; c < 3; ++c)
       if (c < nc && act[c]) y[c] += v * (double)x[c * n + j];
   }
@@ -93,6 +95,7 @@ __device__ __forceinline__ void sell_row3_regs(const DSellT<T>& A, int r, const 
   double v[WM];
   sell_regs<WM>(A.sliceOff, A.col, A.val, r, c, v);
   const double d = (double)A.diag[r];
+#pragma unroll
   for (int q = 0; q < 3; ++q) {
     if (!(q < nc && act[q])) {
       y[q] = 0.0;
@@ -129,7 +132,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgsT<T> a) {
   const int n = a.A.n;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       const size_t o = (size_t)c * n;
       const double bb = (double)a.b[o + r];
       const double rr = bb - sell_row(a.A, r, a.x + o);
@@ -142,7 +145,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgsT<T> a) {
     }
   }
   if (grid_reduce<6>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       double* s = a.sc + 8 * c;
       int* f = a.fl + 4 * c;
       const double bn = sqrt(acc[2 * c + 1]);
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgsT<T> a) {
   const int n = a.A.n;
   double beta[3], om[3];
   bool act[3];
-  for (int c = 0; c < a.nc; ++c) {
+  _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
     const double* s = a.sc + 8 * c;
     act[c] = !a.fl[4 * c];
     beta[c] = (s[1] / s[0]) * (s[2] / s[3]);
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgsT<T> a) {
   }
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const double dinv = 1.0 / (double)a.A.diag[r];
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
       const double pn = (double)a.r[i] + beta[c] * ((double)a.p[i] - om[c] * (double)a.v[i]);
@@ -192,12 +195,12 @@ __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgsT<T> a) {
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
   bool act[3];
-  for (int c = 0; c < a.nc; ++c) act[c] = !a.fl[4 * c];
+  _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) act[c] = !a.fl[4 * c];
   double acc[3] = {0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     double y[3];
     row3<WM>(a.A, r, a.ph, (size_t)n, act, a.nc, y);
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
       a.v[o + r] = (T)y[c];
@@ -205,7 +208,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_v(BicgArgsT<T> a) {
     }
   }
   if (grid_reduce<3>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       double* s = a.sc + 8 * c;
       s[2] = acc[c] != 0.0 ? s[1] / acc[c] : 0.0;
@@ -226,14 +229,14 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgsT<T> a) {
   const int n = a.A.n;
   bool act[3];
   double al[3];
-  for (int c = 0; c < a.nc; ++c) {
+  _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
     act[c] = !a.fl[4 * c];
     al[c] = a.sc[8 * c + 2];
   }
   double acc[3] = {0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const double dinv = 1.0 / (double)a.A.diag[r];
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
       const double sv = (double)a.r[i] - al[c] * (double)a.v[i];
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgsT<T> a) {
     }
   }
   if (grid_reduce<3>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       if (sqrt(acc[c]) <= a.sc[8 * c + 4]) a.fl[4 * c + 1] = 1;
     }
@@ -257,12 +260,12 @@ __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgsT<T> a) {
   if (all_done(a.fl, a.nc)) return;
   const int n = a.A.n;
   bool act[3];
-  for (int c = 0; c < a.nc; ++c) act[c] = !a.fl[4 * c] && !a.fl[4 * c + 1];
+  _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) act[c] = !a.fl[4 * c] && !a.fl[4 * c + 1];
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     double y[3];
     row3<WM>(a.A, r, a.sh, (size_t)n, act, a.nc, y);
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
       const double tv = y[c];
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_t(BicgArgsT<T> a) {
     }
   }
   if (grid_reduce<6>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       a.sc[8 * c + 3] = acc[2 * c + 1] > 0.0 ? acc[2 * c] / acc[2 * c + 1] : 0.0;
     }
@@ -287,7 +290,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgsT<T> a) {
   const int n = a.A.n;
   bool act[3], half[3];
   double al[3], om[3];
-  for (int c = 0; c < a.nc; ++c) {
+  _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
     act[c] = !a.fl[4 * c];
     half[c] = a.fl[4 * c + 1] != 0;
     al[c] = a.sc[8 * c + 2];
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgsT<T> a) {
   }
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
       if (half[c]) {
@@ -310,7 +313,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgsT<T> a) {
     }
   }
   if (grid_reduce<6>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       double* s = a.sc + 8 * c;
       int* f = a.fl + 4 * c;
@@ -877,10 +880,11 @@ __global__ void __launch_bounds__(kBlock) k_defect(DefectArgs a) {
   __shared__ double sm[6 * 32];
   const int n = a.A.n;
   bool act[3];
+#pragma unroll
   for (int c = 0; c < 3; ++c) act[c] = c < a.nc && !(a.frozen && a.frozen[c]);
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t o = (size_t)c * n;
       const double bb = a.b[o + r];
@@ -891,7 +895,7 @@ __global__ void __launch_bounds__(kBlock) k_defect(DefectArgs a) {
     }
   }
   if (grid_reduce<6>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    for (int c = 0; c < a.nc; ++c) {
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) {
         a.fl[4 * c] = 1;
         continue;
