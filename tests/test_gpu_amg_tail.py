@@ -1,7 +1,11 @@
-"""The coarse tail of the AMG V-cycle (the small CSR levels and the dense level run as one
-thread-block-cluster kernel) does the per-level kernels' arithmetic in the same order, so the
-SIMPLE fields must be bit-identical with the tail off, on and covering every CSR level, in FP64 and
-in the mixed-precision method."""
+"""Two launch-saving forms of the AMG V-cycle do the per-level kernels' arithmetic in the same order,
+so the SIMPLE fields must be bit-identical with them on or off, in FP64 and in the mixed-precision
+method:
+
+* the coarse tail: the small CSR levels and the dense level run as one thread-block-cluster kernel
+  (ANB_AMG_TAIL_ROWS: 0 = off, a huge value = every CSR level in the tail);
+* the fused down sweep: down sweep and restriction of a CSR level as one warp-per-aggregate
+  kernel (ANB_AMG_FUSED_DOWN_ROWS: 0 = off, a huge value = every CSR level above the tail)."""
 import os
 
 import numpy as np
@@ -13,11 +17,13 @@ from tests.cases import channel, initial_state
 pytestmark = pytest.mark.gpu
 
 PRM = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3, n_nonorth_corr=1)
+KNOBS = ("ANB_AMG_TAIL_ROWS", "ANB_AMG_FUSED_DOWN_ROWS")
 
 
-def _run(m, bc, init, tail_rows, precision):
-    old = os.environ.get("ANB_AMG_TAIL_ROWS")
+def _run(m, bc, init, precision, tail_rows, fused_rows):
+    old = {k: os.environ.get(k) for k in KNOBS}
     os.environ["ANB_AMG_TAIL_ROWS"] = str(tail_rows)
+    os.environ["ANB_AMG_FUSED_DOWN_ROWS"] = str(fused_rows)
     try:
         s = anb.Solver(m, anb.default_params(precision=precision, **PRM))
         s.set_bc(bc)
@@ -25,20 +31,21 @@ def _run(m, bc, init, tail_rows, precision):
         _, st = s.iterate(6)
         return s.get_state(), st
     finally:
-        if old is None:
-            os.environ.pop("ANB_AMG_TAIL_ROWS")
-        else:
-            os.environ["ANB_AMG_TAIL_ROWS"] = old
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_tail_is_bit_identical(precision):
+def test_launch_saving_forms_are_bit_identical(precision):
     # 36k cells: five or six levels, so 3000 rows splits the CSR levels between launches and tail
     m, bc, _ = channel(nx=60, ny=25, nz=24, jitter=0.15, seed=3, obstacle=True)
     init = initial_state(m, bc)
-    ref, st0 = _run(m, bc, init, 0, precision)
-    for rows in (3000, 1 << 30):
-        got, st = _run(m, bc, init, rows, precision)
-        assert [x["its_p_total"] for x in st] == [x["its_p_total"] for x in st0], rows
+    ref, st0 = _run(m, bc, init, precision, 0, 0)
+    for tail, fused in ((3000, 0), (1 << 30, 0), (0, 1 << 30), (3000, 1 << 30), (1024, 65536)):
+        got, st = _run(m, bc, init, precision, tail, fused)
+        assert [x["its_p_total"] for x in st] == [x["its_p_total"] for x in st0], (tail, fused)
         for k in ("u", "v", "w", "p", "phi"):
-            assert np.array_equal(got[k], ref[k]), (rows, k)
+            assert np.array_equal(got[k], ref[k]), (tail, fused, k)
