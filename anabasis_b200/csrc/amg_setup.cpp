@@ -148,6 +148,8 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
   {
     AmgLevelHost lv0;
     lv0.n = A.n;
+    lv0.nStore = L.sliceOff.back();
+    lv0.maxW = L.maxRowLen;
     levels.push_back(std::move(lv0));  // pattern comes from the mesh layout
   }
   while ((int)levels.size() < opt.maxLevels && A.n > opt.coarseMax) {
@@ -181,10 +183,41 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
     }
     AmgLevelHost coarse;
     coarse.n = nc;
-    coarse.rowOff = Cc.off;
-    coarse.col = Cc.col;
-    // gather lists: coarse CSR entries then coarse diagonals
-    const int nEnt = Cc.off[nc];
+    // storage slot of every coarse CSR entry (identity for a CSR level)
+    std::vector<int> slot(Cc.off[nc]);
+    if (nc > std::max(opt.sellMinRows, 4 * opt.coarseMax)) {
+      const int nSl = (nc + kSlice - 1) / kSlice;
+      coarse.sliceOff.assign(nSl + 1, 0);
+      for (int sl = 0; sl < nSl; ++sl) {
+        int w = 0;
+        for (int I = sl * kSlice; I < std::min(nc, (sl + 1) * kSlice); ++I) w = std::max(w, Cc.off[I + 1] - Cc.off[I]);
+        coarse.maxW = std::max(coarse.maxW, w);
+        coarse.sliceOff[sl + 1] = coarse.sliceOff[sl] + w * kSlice;
+      }
+      coarse.nStore = coarse.sliceOff[nSl];
+      coarse.col.assign(coarse.nStore, 0);
+      for (int I = 0; I < nc; ++I) {
+        const int sl = I / kSlice, lane = I % kSlice;
+        const int w = (coarse.sliceOff[sl + 1] - coarse.sliceOff[sl]) / kSlice;
+        for (int k = 0; k < w; ++k) {
+          const int e = coarse.sliceOff[sl] + k * kSlice + lane;
+          const int kk = Cc.off[I] + k;
+          if (kk < Cc.off[I + 1]) {
+            coarse.col[e] = Cc.col[kk];
+            slot[kk] = e;
+          } else {
+            coarse.col[e] = I;  // padding: the row itself, value 0
+          }
+        }
+      }
+    } else {
+      coarse.rowOff = Cc.off;
+      coarse.col = Cc.col;
+      coarse.nStore = Cc.off[nc];
+      for (int k = 0; k < Cc.off[nc]; ++k) slot[k] = k;
+    }
+    // gather lists: coarse storage slots (padding slots get empty lists) then coarse diagonals
+    const int nEnt = coarse.nStore;
     std::vector<int> cnt(nEnt + nc + 1, 0);
     std::vector<int> target(A.off[A.n]);
     for (int i = 0; i < A.n; ++i) {
@@ -196,7 +229,7 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
           t = nEnt + I;
         } else {
           const auto b = Cc.col.begin() + Cc.off[I], e = Cc.col.begin() + Cc.off[I + 1];
-          t = (int)(std::lower_bound(b, e, J) - Cc.col.begin());
+          t = slot[(int)(std::lower_bound(b, e, J) - Cc.col.begin())];
         }
         target[k] = t;
         cnt[t + 1]++;
@@ -214,10 +247,9 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
       }
     }
     levels.push_back(std::move(coarse));
-    // the coarse level is stored as CSR: its storage index is the CSR index
+    // storage index of each CSR entry of the new fine level
     A = std::move(Cc);
-    storage.resize(A.off[A.n]);
-    for (int k = 0; k < A.off[A.n]; ++k) storage[k] = k;
+    storage = std::move(slot);
   }
   return levels;
 }

@@ -20,9 +20,14 @@ namespace anb {
 
 struct AmgLevelHost {
   int n = 0;
-  // CSR off-diagonal pattern of this level (levels >= 1; level 0 uses the mesh layout's SELL-32
-  // pattern).  Coarse rows are long and few, so the device walks them with several lanes per row.
-  std::vector<int> rowOff, col;
+  // Off-diagonal pattern of this level (levels >= 1; level 0 uses the mesh layout's SELL-32
+  // pattern).  Large coarse levels are SELL-32 like level 0 (sliceOff: slices of 32 rows, slot k of
+  // row r at sliceOff[r/32] + 32k + r%32, padding slots point at the row itself with value 0) and
+  // run the level-0 kernels, thread per row; small ones are CSR (rowOff), whose rows are walked by
+  // several lanes each.  nStore is the number of value slots either way.
+  std::vector<int> rowOff, sliceOff, col;
+  int nStore = 0;
+  int maxW = 0;  // SELL: largest slice width
   // restriction to the next level (empty on the coarsest level)
   int nc = 0;
   std::vector<int> agg;            // n: aggregate (coarse row) of each row
@@ -41,6 +46,8 @@ struct AmgSetupOptions {
   // pairwise passes for the coarsening of level l (l = 0, 1, ...); the last entry repeats, and an
   // empty list means passesPerLevel everywhere
   std::vector<int> passes;
+  // coarse levels with more rows than this are stored SELL-32, smaller ones CSR
+  int sellMinRows = 65536;
 };
 
 // vals / diag are the level-0 matrix in the layout's SELL-32 storage.

@@ -250,6 +250,7 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
   CK(cudaMemcpyAsync(hd.data(), diag0, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   AmgSetupOptions opt;
+  if (const char* sr = std::getenv("ANB_AMG_SELL_MIN_ROWS")) opt.sellMinRows = std::atoi(sr);
   if (const char* ps = std::getenv("ANB_AMG_PASSES")) {  // e.g. "2,2,3": passes per level
     for (const char* q = ps; *q;) {
       opt.passes.push_back(std::max(1, std::atoi(q)));
@@ -275,9 +276,14 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
       d.wdinv = wdinv0;
       d.maxW = c->L.maxRowLen;
     } else {
-      d.rowOff = ar.upload(h.rowOff);
+      if (!h.sliceOff.empty()) {
+        d.sliceOff = ar.upload(h.sliceOff);
+        d.maxW = h.maxW;
+      } else {
+        d.rowOff = ar.upload(h.rowOff);
+      }
       d.col = ar.upload(h.col);
-      d.val = ar.alloc<T>(h.rowOff.back());
+      d.val = ar.alloc<T>(std::max(h.nStore, 1));
       d.diag = ar.alloc<T>(h.n);
       d.b = ar.alloc<T>(h.n);
       d.wdinv = ar.alloc<T>(h.n);
@@ -290,7 +296,7 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
       d.mem = ar.upload(h.mem);
       d.gOff = ar.upload(h.gOff);
       d.gIdx = ar.upload(h.gIdx);
-      d.nEntNext = c->amgHost[l + 1].rowOff.back();
+      d.nEntNext = c->amgHost[l + 1].nStore;
     }
   }
   const int nd = c->amgHost.back().n;

@@ -238,8 +238,8 @@ using PcgArgs = PcgArgsT<double>;
 template <class T>
 struct AmgLevelDevT {
   int n, nc;
-  // matrix of this level: level 0 borrows the pressure matrix (SELL-32 slices in sliceOff),
-  // coarser levels are CSR (rowOff)
+  // matrix of this level: level 0 borrows the pressure matrix (SELL-32 slices in sliceOff); large
+  // coarse levels are SELL-32 too (sliceOff, run by the level-0 kernels), small ones CSR (rowOff)
   const int* sliceOff;
   const int* rowOff;
   const int* col;

@@ -969,7 +969,9 @@ static int tail_start(const AmgDevT<T>* amg) {
   const int L = amg->nLevels;
   if (amg->tailCluster <= 0 || amg->tailRows <= 0) return L - 1;
   int t0 = L - 1;
-  while (t0 - 1 >= 1 && amg->lv[t0 - 1].n <= amg->tailRows && L - (t0 - 1) <= kTailMaxLevels) --t0;
+  while (t0 - 1 >= 1 && amg->lv[t0 - 1].n <= amg->tailRows && !amg->lv[t0 - 1].sliceOff &&
+         L - (t0 - 1) <= kTailMaxLevels)
+    --t0;
   return t0;
 }
 
@@ -1036,12 +1038,22 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
   }
   {
     const int t0 = tail_start(amg);
+    auto fused = [&](const AmgLevelDevT<T>& f) { return !f.sliceOff && f.n <= amg->fusedDownRows; };
     int nl = 1;
-    for (int l = 1; l < t0; ++l) nl += 2 + (amg->lv[l].n > amg->fusedDownRows ? 1 : 0);
+    for (int l = 1; l < t0; ++l) nl += fused(amg->lv[l]) ? 2 : 3;
     ProfScope ps(lc, kKfAmgCoarse, 0.0, nl);
     for (int l = 1; l < t0; ++l) {
       const AmgLevelDevT<T>& f = amg->lv[l];
-      if (f.n <= amg->fusedDownRows) {
+      if (f.sliceOff) {  // large coarse level in SELL-32: the level-0 kernels, thread per row
+        const int wc = sell_width_class(f.maxW);
+        const int nb = blocks_for(f.n, lc.rowBlocks);
+        if (wc == 4) k_amg_resid<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+        else if (wc == 8) k_amg_resid<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+        else k_amg_resid<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+        k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
+        continue;
+      }
+      if (fused(f)) {
         k_amg_down_csr<kCoarseLanes, T><<<blocks_for(f.nc * 32, lc.rowBlocks), kBlock, 0, lc.stream>>>(
             a.fl, f, amg->lv[l + 1].b);
         continue;
@@ -1060,6 +1072,14 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
       const AmgLevelDevT<T>& f = amg->lv[l];
       // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
       const T* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
+      if (f.sliceOff) {
+        const int wc = sell_width_class(f.maxW);
+        const int nb = blocks_for(f.n, lc.rowBlocks);
+        if (wc == 4) k_amg_up<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
+        else if (wc == 8) k_amg_up<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
+        else k_amg_up<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
+        continue;
+      }
       k_amg_up_csr<kCoarseLanes, T><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
           a.fl, f, e, amg->omega, amg->corr, f.x2);
     }
