@@ -422,7 +422,7 @@ def run_adjoint1m(args) -> dict:
 def run_tets16m(args) -> dict:
     """Config 5: 463x76x76 jittered hexes (seed 2) split into 6 tets, obstacle removed before the
     split (~16M cells).  Mixed-precision forward for --steps SIMPLE steps from the initial state,
-    the same steps in FP64 as the accuracy judge, then the adjoint gradient of the obstacle force at
+    the same steps in FP64 as the accuracy reference, then the adjoint gradient of the obstacle force at
     the FP64 state restored from a host checkpoint of (U, p) in a fresh FP64 context; peak device
     memory of each phase."""
     import anabasis_b200 as anb

@@ -12,7 +12,7 @@
  *     /root/reference by oracle/build_ref.sh (tests/test_oracle_vs_reference.py);
  *   - the linear solves of the reference are HYPRE 3.0.0 (not vendored, not installable here):
  *     the oracle replaces them with deterministic FP64 Krylov solvers run to tight tolerance, so
- *     solver-level parity is unpinned and parity is judged on converged/tightly-solved fields.
+ *     solver-level parity is unpinned and parity is checked on converged/tightly-solved fields.
  */
 #ifndef ANB_ORACLE_H
 #define ANB_ORACLE_H
