@@ -278,10 +278,20 @@ class Solver:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p)]
         self._check(lib().anb_set_state(self._h, *map(_d, arrs)))
 
-    def get_state(self, with_phi: bool = True) -> dict:
+    def get_state(self, with_phi: bool = True, out: dict | None = None) -> dict:
+        """Fields in input numbering.  `out` (a dict returned by an earlier call) is filled in place,
+        which spares a caller that reads the state every step the allocation and first-touch page
+        faults of fresh arrays."""
         C, F = self.n_cells, self.n_faces
-        o = dict(u=np.zeros(C), v=np.zeros(C), w=np.zeros(C), p=np.zeros(C))
-        o["phi"] = np.zeros(F) if with_phi else None
+        o = out if out is not None else dict(u=np.zeros(C), v=np.zeros(C), w=np.zeros(C), p=np.zeros(C))
+        if with_phi and o.get("phi") is None:
+            o["phi"] = np.zeros(F)
+        elif not with_phi:
+            o["phi"] = None
+        for k, n in (("u", C), ("v", C), ("w", C), ("p", C)) + ((("phi", F),) if with_phi else ()):
+            a = o[k]
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous and a.size == n):
+                raise ValueError(f"out[{k!r}] must be a contiguous float64 array of {n} values")
         self._check(lib().anb_get_state(self._h, _d(o["u"]), _d(o["v"]), _d(o["w"]), _d(o["p"]), _d(o["phi"])))
         return o
 
