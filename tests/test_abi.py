@@ -1,7 +1,11 @@
 """The C ABI: libanb.so loads and exports every function include/*.h declares (no GPU needed)."""
 import ctypes as ct
 import re
+import types
 from pathlib import Path
+
+import numpy as np
+import pytest
 
 import anabasis_b200 as anb
 import oracle
@@ -46,3 +50,24 @@ def test_library_entry_points_without_gpu():
 
 def test_oracle_loads():
     assert oracle.lib() is not None
+
+
+def test_get_state_refills_caller_arrays(monkeypatch):
+    """Solver.get_state(out=...) hands the caller's arrays to anb_get_state (no GPU: the library call
+    is replaced by a recorder) and rejects arrays of the wrong size."""
+    seen = []
+
+    class Recorder:
+        def anb_get_state(self, h, u, v, w, p, phi):
+            seen.append((u, phi))
+            return 0
+
+    monkeypatch.setattr(anb, "lib", lambda: Recorder())
+    fake = types.SimpleNamespace(n_cells=5, n_faces=7, _h=None, _check=lambda rc: None)
+    first = anb.Solver.get_state(fake)
+    assert first["u"].shape == (5,) and first["phi"].shape == (7,)
+    again = anb.Solver.get_state(fake, with_phi=False, out=first)
+    assert again is first and again["phi"] is None
+    assert seen[1][0].contents is not None and seen[1][1] is None
+    with pytest.raises(ValueError):
+        anb.Solver.get_state(fake, out=dict(u=np.zeros(4), v=np.zeros(5), w=np.zeros(5), p=np.zeros(5)))
