@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -56,13 +57,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     LIB.mkdir(exist_ok=True)
     hdrs = _headers()
     objs: list[Path] = []
+    jobs: list[list[str]] = []
     for src in HOST_SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".o")
         if force or _stale(o, [s] + hdrs):
             if verbose:
                 print("g++", src)
-            _run(["g++", *CXXFLAGS, f"-I{CUDA_HOME}/include", "-c", str(s), "-o", str(o)])
+            jobs.append(["g++", *CXXFLAGS, f"-I{CUDA_HOME}/include", "-c", str(s), "-o", str(o)])
         objs.append(o)
     for src in CUDA_SOURCES:
         s = CSRC / src
@@ -70,8 +72,12 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if force or _stale(o, [s] + hdrs):
             if verbose:
                 print("nvcc", src)
-            _run([NVCC, *NVCCFLAGS, "-c", str(s), "-o", str(o)])
+            jobs.append([NVCC, *NVCCFLAGS, "-c", str(s), "-o", str(o)])
         objs.append(o)
+    # translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j) for j in jobs]:
+            f.result()
     lib = LIB / "libanb.so"
     if force or _stale(lib, objs):
         _run([NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-Xcompiler", "-fopenmp", "-lgomp"])

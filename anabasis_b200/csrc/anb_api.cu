@@ -541,8 +541,9 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   int its[3] = {0, 0, 0};
   {
     const int nVel = std::max(p.n_vel_nonorth_corr, 0) + 1;
+    if (nVel > 1 && !c->UsPrev)
+      throw AnbError(ANB_ERR_INVALID, "n_vel_nonorth_corr changed after anb_create");
     int active[3] = {1, 1, 1};
-    std::vector<double> qPrev;
     for (int it = 1; it <= nVel; ++it) {
       if (it > 1) {
         // rhs-only re-assembly on the current iterates (K26, K9, K7, K8, K10)
@@ -553,11 +554,8 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
         launch_mom(c, c->Us, 1);
       }
       // keep the iterate for the relative-change test (main.cu:3377-3381)
-      std::vector<double> before;
-      if (nVel > 1) {
-        before.resize((size_t)3 * C);
-        CK(cudaMemcpyAsync(before.data(), c->Us, sizeof(double) * 3 * C, cudaMemcpyDeviceToHost, c->stream));
-      }
+      if (nVel > 1 && it < nVel)
+        CK(cudaMemcpyAsync(c->UsPrev, c->Us, sizeof(double) * 3 * C, cudaMemcpyDeviceToDevice, c->stream));
       int itq[3];
       bool cv[3];
       solve_momentum(c, active, itq, cv);
@@ -567,19 +565,12 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
           anyNC = anyNC || !cv[q];
         }
       if (nVel > 1 && it < nVel) {
-        std::vector<double> after((size_t)3 * C);
-        CK(cudaMemcpyAsync(after.data(), c->Us, sizeof(double) * 3 * C, cudaMemcpyDeviceToHost, c->stream));
+        // relchg = sqrt(sum (q_new - q_iter)^2 / (1 + sum q_new^2)) per component, reduced on the device
+        launch_relchg3(c->lc, C, c->UsPrev, c->Us, c->red, c->scal + kScalRelchg);
+        CK(cudaMemcpyAsync(c->hScal, c->scal + kScalRelchg, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
-        for (int q = 0; q < 3; ++q) {
-          if (!active[q]) continue;
-          double num = 0.0, den = 1.0;
-          for (int r = 0; r < C; ++r) {
-            const double d = after[(size_t)q * C + r] - before[(size_t)q * C + r];
-            num += d * d;
-            den += after[(size_t)q * C + r] * after[(size_t)q * C + r];
-          }
-          if (std::sqrt(num / den) < p.corr_tol) active[q] = 0;
-        }
+        for (int q = 0; q < 3; ++q)
+          if (active[q] && std::sqrt(c->hScal[2 * q] / (1.0 + c->hScal[2 * q + 1])) < p.corr_tol) active[q] = 0;
         if (!active[0] && !active[1] && !active[2]) break;
       }
     }
@@ -587,8 +578,12 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   // 3. pressure matrix + Rhie-Chow flux + continuity, p' = 0
   if (c->mixed) launch_prc<float>(c, c->pval32, c->pdiag32, c->pwdinv32);
   else launch_prc<double>(c, c->pval, c->pdiag, c->pwdinv);
+  // preconditioner refresh: at the rebuild cadence (main.cu:3409-3411), or before every pressure
+  // solve with pAmgSetupScope 1 (main.cu:2594-2598; the fine matrix does not change between the
+  // solves of one step, so the later refreshes reproduce the same hierarchy values)
   const int every = std::max(p.p_amg_rebuild_every, 1);
-  if (!c->amgBuilt || c->outerStep == 1 || ((c->outerStep - 1) % every) == 0) ensure_amg(c);
+  const bool perSolve = p.p_amg_setup_scope == 1;
+  if (perSolve || !c->amgBuilt || c->outerStep == 1 || ((c->outerStep - 1) % every) == 0) ensure_amg(c);
   // 4. non-orthogonal pressure passes
   const int nPS = std::max(p.n_nonorth_corr, 0) + 1, nExtra = std::max(p.n_pressure_corr, 0);
   const int total = nPS + nExtra;
@@ -618,6 +613,7 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
     ++counter;
     const double rtol = counter == total ? 0.0 : p.p_rel_tol;
     bool cv = true;
+    if (perSolve && pc > 1) ensure_amg(c);
     solve_pressure(c, c->pb, c->Pc, rtol, &pLast, &cv);
     anyNC = anyNC || !cv;
     pTot += pLast;
@@ -631,24 +627,15 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   }
   for (int k = 1; k <= nExtra; ++k) {  // main.cu:3521-3567
     // b = -divCorr ; dp' from zero ; p' += dp'
-    std::vector<double> h(C);
-    CK(cudaMemcpyAsync(h.data(), c->divCorr, sizeof(double) * C, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (double& v : h) v = -v;
-    CK(cudaMemcpyAsync(c->pb, h.data(), sizeof(double) * C, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(c->pdx, 0, sizeof(double) * C, c->stream));
+    launch_pass_rhs(c->lc, C, c->divCorr, c->pb, c->pdx);
     ++counter;
     const double rtol = counter == total ? 0.0 : p.p_rel_tol;
     bool cv = true;
+    if (perSolve) ensure_amg(c);
     solve_pressure(c, c->pb, c->pdx, rtol, &pLast, &cv);
     anyNC = anyNC || !cv;
     pTot += pLast;
-    std::vector<double> hp(C), hd(C);
-    CK(cudaMemcpyAsync(hp.data(), c->Pc, sizeof(double) * C, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(hd.data(), c->pdx, sizeof(double) * C, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    for (int r = 0; r < C; ++r) hp[r] += 1.0 * hd[r];
-    CK(cudaMemcpyAsync(c->Pc, hp.data(), sizeof(double) * C, cudaMemcpyHostToDevice, c->stream));
+    launch_add_scaled(c->lc, C, 1.0, c->pdx, c->Pc);
     const double* phi[1] = {c->Pc};
     double* out[1] = {c->Gc};
     grad(c, 1, phi, pbit, out);
@@ -796,6 +783,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
 
     CK(cudaSetDevice(prm->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    if (nalloc_prepare_device(prm->device) != 0)
+      throw AnbError(ANB_ERR_CUDA, "could not place the static scratch of anb_patch_force_nalloc on the device");
     int nSM = 148;
     CK(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, prm->device));
     c->lc.stream = c->stream;
@@ -928,6 +917,9 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       c->pwdinv = A.alloc<double>(C);
     }
     c->pdx = A.alloc<double>(C);
+    if (prm->n_vel_nonorth_corr > 0) c->UsPrev = A.alloc<double>(3 * C);
+    if (prm->p_amg_setup_scope != 0 && prm->p_amg_setup_scope != 1)
+      throw AnbError(ANB_ERR_INVALID, "p_amg_setup_scope must be 0 (outer) or 1 (pressure)");
     if (const char* s = std::getenv("ANB_AMG_OMEGA")) c->amg.omega = std::atof(s);
     if (const char* s = std::getenv("ANB_AMG_CORR")) c->amg.corr = std::atof(s);
     c->amg32.omega = c->amg.omega;

@@ -324,6 +324,7 @@ int main(int argc, char** argv) {
   prm.corr_tol = par.corrTol;
   prm.p_amg_rebuild_every = par.pAmgRebuildEvery;
   prm.p_use_amg = par.p_use_amg;
+  prm.p_amg_setup_scope = par.pAmgSetupScope;
   prm.precision = par.precision;
   prm.device = par.device;
   std::vector<double> pts((size_t)3 * mesh.nPoints());

@@ -92,6 +92,7 @@ struct anb_ctx {
   double *mval = nullptr, *mdiag = nullptr, *rhs = nullptr;
   double *pval = nullptr, *pdiag = nullptr, *pb = nullptr, *divStar = nullptr, *divCorr = nullptr;
   double *phiStar = nullptr, *phi = nullptr;
+  double* UsPrev = nullptr;   // momentum iterates before a re-solve (3*C; only with nVelNonOrthCorr > 0)
   double *bw[8] = {nullptr};  // BiCGSTAB work vectors (3*C each)
   double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pq = nullptr, *pdx = nullptr;
   double* pwdinv = nullptr;   // omega / pressure diagonal (level-0 smoother)
@@ -138,6 +139,7 @@ constexpr int kScalBicg = 0;    // 3 * 8
 constexpr int kScalPcg = 24;    // 8
 constexpr int kFlagBicg = 0;    // 3 * 4
 constexpr int kFlagPcg = 12;    // 4
+constexpr int kScalRelchg = 56; // 6: momentum relative-change sums
 
 int fail(anb_ctx* c, const AnbError& e);
 

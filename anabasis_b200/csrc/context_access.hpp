@@ -25,5 +25,8 @@ struct ForceView {
 // Returns false when `patch` is not a patch of the context's mesh.
 bool context_force_view(const anb_ctx* c, int patch, ForceView* v);
 void context_set_error(anb_ctx* c, const char* msg);
+// Places the allocation-free force integral's static scratch and kernel on `device` (the current
+// device); returns 0 on success.  Called by anb_create.
+int nalloc_prepare_device(int device);
 
 }  // namespace anb

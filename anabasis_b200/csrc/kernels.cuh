@@ -193,6 +193,13 @@ struct FluxArgs {
 };
 void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a);
 
+// Extra pressure passes: b = -divCorr and dx = 0; y += s x.
+void launch_pass_rhs(const LaunchCfg& lc, int n, const double* divCorr, double* b, double* dx);
+void launch_add_scaled(const LaunchCfg& lc, int n, double s, const double* x, double* y);
+// out[2q], out[2q+1] = sum (after_q - before_q)^2, sum after_q^2 over n rows, q = 0..2 (device)
+void launch_relchg3(const LaunchCfg& lc, int n, const double* before, const double* after, Reducer red,
+                    double* out);
+
 // Patch force (compute_patch_forces_wall_shear, main.cu:2828-2933) over boundary faces
 // [b0, b1); out: Fp[3] Fv[3] F[3] area nFaces minDn maxDn maxUt maxShear (15 doubles).
 void launch_patch_force(cudaStream_t s, const DMesh& m, int b0, int b1, int sign, double mu,

@@ -541,7 +541,55 @@ __global__ void k_patch_force(DMesh m, int b0, int b1, int sign, double mu, cons
   }
 }
 
+// ---- extra pressure passes (nPressureCorr, main.cu:3521-3567) ------------------------------
+// b = -divCorr (kernel_build_pressure_rhs_minus_div, main.cu:1606-1613; the reference's pressure
+// anchor is off, main.cu:3294) and dp' = 0 for the pass's solve from zero.
+__global__ void __launch_bounds__(kBlock) k_pass_rhs(int n, const double* divCorr, double* b, double* dx) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    b[i] = -divCorr[i];
+    dx[i] = 0.0;
+  }
+}
+
+// y += s x (kernel_add_scaled_inplace, main.cu:1442-1445)
+__global__ void __launch_bounds__(kBlock) k_add_scaled(int n, double s, const double* x, double* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += s * x[i];
+}
+
+// Relative change of the three momentum iterates (main.cu:3377-3379): per component the sum of
+// (after - before)^2 and of after^2, combined in block order into out[0..5].
+__global__ void __launch_bounds__(kBlock) k_relchg3(int n, const double* before, const double* after, Reducer red,
+                                                    double* out) {
+  __shared__ double sm[6 * 32];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double a = after[(size_t)q * n + i];
+      const double d = a - before[(size_t)q * n + i];
+      acc[2 * q] += d * d;
+      acc[2 * q + 1] += a * a;
+    }
+  }
+  if (grid_reduce<6>(acc, 0u, red, sm) && threadIdx.x == 0)
+    for (int q = 0; q < 6; ++q) out[q] = acc[q];
+}
+
 }  // namespace
+
+void launch_pass_rhs(const LaunchCfg& lc, int n, const double* divCorr, double* b, double* dx) {
+  g_launches += 1;
+  k_pass_rhs<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(n, divCorr, b, dx);
+}
+void launch_add_scaled(const LaunchCfg& lc, int n, double s, const double* x, double* y) {
+  g_launches += 1;
+  k_add_scaled<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(n, s, x, y);
+}
+void launch_relchg3(const LaunchCfg& lc, int n, const double* before, const double* after, Reducer red,
+                    double* out) {
+  g_launches += 1;
+  k_relchg3<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(n, before, after, red, out);
+}
 
 std::atomic<long long> g_launches{0};
 

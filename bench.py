@@ -7,7 +7,12 @@ Workload (one "step" = one steady SIMPLE outer iteration of the reference's gene
   (970,480 cells, 2,876,926 internal faces), parabolic inlet Umax 0.45, fixed-p outlet, no-slip
   walls and obstacle, rho 1, mu 1e-3, relaxation U 0.7 / p 0.3, 2 non-orthogonal correctors,
   FP64 plain method, inner tolerances 1e-10 absolute (the reference defaults).
-  The mesh and fields are synthetic (generated here); device working set ~1.5 GB > 126 MB L2.
+  The mesh and fields are synthetic (generated here); device working set ~1.9 GB > 126 MB L2.
+
+Reference arm (--impl reference): the CPU oracle (oracle/, a C++/OpenMP restatement of the
+reference's SIMPLE iteration; the reference's own HYPRE path cannot be built without HYPRE and MPI)
+on the box's host cores, same case built by the oracle alone (no product library in the process),
+same warm-up and timed step indices as the library arm.
 
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -33,11 +38,11 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = dict(nx=200, ny=70, nz=70, jitter=0.15, seed=0, obstacle=True)
 PARAMS = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3, n_nonorth_corr=2)
-KERNEL_FAMILY = 7  # ANB_KF_PCG_SPMV: the dominant kernel of the step (see profiles/)
+KERNEL_FAMILY = 7  # ANB_KF_PCG_SPMV: the largest bandwidth-bound kernel of the step
 # DRAM bytes (read + write) per k_pcg_pq launch on this workload: mean of 3 launches of
 #   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
 #       -k regex:k_pcg_pq -s 30 -c 3 python bench.py --steps 2 --warmup 3 --no-cpu
-# (93.10 MB read + 3.18 MB write; profiles/k_pcg_pq_obstacle1m.md)
+# (93.10 MB read + 3.18 MB write)
 PCG_SPMV_TRAFFIC_BYTES = 96.29e6
 FAMILY_NAMES = {1: "k_lsq_grad", 2: "k_momentum", 3: "k_pressure_rc", 4: "k_nonorth_rhs", 5: "k_flux_final",
                 6: "k_bicg_v/k_bicg_t", 7: "k_pcg_pq"}
@@ -153,6 +158,14 @@ def make_case():
     return m, bc, initial_state(m, bc)
 
 
+def bench_config(world: int) -> dict:
+    """The `config` of both arms' JSON lines (the same workload, so the same dict)."""
+    return {"workload": "obstacle channel 200x70x70 jittered hex (970480 cells), FP64 SIMPLE, "
+                        "2 non-orthogonal correctors, inner tol 1e-10",
+            "cells": 970480, "internal_faces": 2876926, "parallelism": f"replicas{world}",
+            "l2": "working set > L2 (no flush needed)"}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     import anabasis_b200 as anb
 
@@ -219,10 +232,8 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "obstacle channel 200x70x70 jittered hex (970480 cells), FP64 SIMPLE, "
-                               "2 non-orthogonal correctors, inner tol 1e-10",
-                   "cells": C, "internal_faces": m.n_internal, "parallelism": f"replicas{world}",
-                   "l2": "working set > L2 (no flush needed)", "wall_seconds_timed": wall},
+        "config": bench_config(world),
+        "wall_seconds_timed": wall,
         "e2e": {"value": replica_throughput(world, C, e2e_steps, e2e_wall), "unit": "cell-iters/s",
                 "h2d_bytes_per_step": 4 * 8 * C, "d2h_bytes_per_step": 4 * 8 * C},
         "gpu_launches": int(launches),
@@ -262,32 +273,35 @@ def cpu_baseline(m, bc, state, steps: int = 1) -> dict:
                       f"({dt:.1f} s)"}
 
 
-def run_reference(args, rank: int) -> dict | None:
+def run_reference(args, rank: int, world: int) -> dict | None:
+    """The oracle port on the host cores: the case is built by the oracle alone (its own channel
+    generator and boundary evaluation, pinned bit for bit to the library's and the reference's),
+    then the same warm-up steps and the same timed steps as the library arm, all host threads."""
     if rank != 0:
         return None
-    m, bc, state = make_case()
-    steps = max(1, min(args.steps, 3))
-    warm = 1 if args.warmup > 0 else 0
     import oracle
 
+    o, bc, state = oracle.channel_case(**WORKLOAD)
     nthreads = os.cpu_count() or 1
-    o = oracle.Oracle(m.topology())
-    o.set_bc(bc)
-    prm = oracle.params(n_threads=nthreads, **PARAMS)
-    s, _ = o.run(prm, warm, *state) if warm else ({"u": state[0], "v": state[1], "w": state[2], "p": state[3]}, None)
+    prm = oracle.params(n_threads=nthreads, tol_mass=0.0, tol_vel=0.0, **PARAMS)  # no early stop
+    s = {"u": state[0], "v": state[1], "w": state[2], "p": state[3]}
+    if args.warmup > 0:
+        s, _ = o.run(prm, args.warmup, *state)
     t0 = time.perf_counter()
-    o.run(prm, steps, s["u"], s["v"], s["w"], s["p"])
+    _, st = o.run(prm, args.steps, s["u"], s["v"], s["w"], s["p"])
     dt = time.perf_counter() - t0
-    v = m.n_cells * steps / dt
+    assert len(st) == args.steps
+    v = o.n_cells * args.steps / dt
     return {
-        "impl": "reference", "metric": "SIMPLE cell-iters/s", "value": v, "unit": "cell-iters/s", "n_gpus": 0,
-        "steps": steps, "warmup": warm, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+        "impl": "reference", "metric": "SIMPLE cell-iters/s", "value": v, "unit": "cell-iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "obstacle channel 200x70x70 jittered hex (970480 cells), FP64 SIMPLE, "
-                               "2 non-orthogonal correctors, inner tol 1e-10", "cells": m.n_cells},
+        "config": bench_config(world),
         "cpu_baseline": {"value": v, "unit": "cell-iters/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{steps} SIMPLE step(s) after {warm} warm-up step(s); the reference's HYPRE "
-                                   f"path cannot be built (no HYPRE/MPI), the oracle port stands in"},
+                         "sample": f"steps {args.warmup + 1}-{args.warmup + args.steps} of the workload (the "
+                                   f"library arm's timed steps) after {args.warmup} warm-up steps; the "
+                                   f"reference's HYPRE path cannot be built (no HYPRE/MPI), the oracle port "
+                                   f"(Jacobi-PCG / Jacobi-BiCGSTAB) stands in"},
         "e2e": {"value": v, "unit": "cell-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -479,14 +493,14 @@ def main():
     ap.add_argument("--dirs", type=int, default=8, help="adjoint1m: finite-difference directions")
     ap.add_argument("--tl-dirs", type=int, default=4, help="adjoint1m: tangent-linear directions")
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    if args.warmup < 3:  # both arms: at least 3 warm-up steps, the same steps timed
         args.warmup = 3
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     studies = {"mixed4m": run_mixed4m, "adjoint1m": run_adjoint1m, "tets16m": run_tets16m}
     if args.impl == "reference":
-        out = run_reference(args, rank)
+        out = run_reference(args, rank, world)
     elif args.config in studies:
         out = studies[args.config](args) if rank == 0 else None
     else:

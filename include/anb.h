@@ -70,6 +70,8 @@ typedef struct anb_params {
   int p_use_amg;             /* 1: aggregation-AMG preconditioned CG, 0: Jacobi CG       */
   int precision;             /* ANB_PRECISION_FP64 or ANB_PRECISION_MIXED                */
   int device;
+  int p_amg_setup_scope;     /* pAmgSetupScope (main.cu:89, 2594-2598): 0 refresh the pressure
+                                preconditioner at the rebuild cadence, 1 before every pressure solve */
 } anb_params;
 
 /* Per-outer-iteration monitor values (the stdout line of main.cu:3609-3611). */
@@ -133,12 +135,14 @@ int anb_patch_force(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* 
  * ask for it (an application that owns the whole GPU through its own pool, code running while
  * another component records a CUDA graph, a plugin with a fixed memory budget).  No counterpart
  * in the reference.  The call allocates nothing: its scratch (block partial sums, result,
- * arrival counter) is one file-scope __device__ array of 131,216 bytes that every GPU loading
- * the library keeps until the process exits.  Limit: patches of at most 262,144 faces
- * (ANB_ERR_INVALID beyond).  The first call on a device looks up the array's device address
- * and clears its counter; make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU (several threads or contexts on one device at once)
- * race and must be serialised by the caller. */
+ * arrival counter) is one file-scope __device__ array of 131,216 bytes.  anb_create places it
+ * (and the kernel's code) on the context's device, while allocation is still allowed, and the
+ * device keeps it until the process exits.  Limit: one face per thread over the array's 1,024
+ * block partials, i.e. patches of at most 262,144 faces (ANB_ERR_INVALID beyond).  Each call
+ * clears the counter and result slots on the context's stream before its launch.  All calls
+ * share the array: calls that overlap on the GPU (several threads or contexts on one device at
+ * once) race and must be serialised by the caller; an overlap that leaves the result unwritten
+ * is reported as ANB_ERR_CUDA.  The caller's current device is restored on return. */
 int anb_patch_force_nalloc(anb_ctx* ctx, int patch, int normal_sign, anb_force_report* out);
 
 /* ---- scalar libraries (method-of-manufactured-solutions path) --------------------------------

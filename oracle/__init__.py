@@ -47,6 +47,14 @@ def lib() -> ct.CDLL:
         L.orc_mesh_free.argtypes = [ct.c_void_p]
         L.orc_mesh_ncells.restype = ct.c_int
         L.orc_mesh_ncells.argtypes = [ct.c_void_p]
+        L.orc_mesh_sizes.argtypes = [ct.c_void_p, _ip]
+        L.orc_mesh_patches.argtypes = [ct.c_void_p, _ip, _ip]
+        L.orc_mesh_topology.argtypes = [ct.c_void_p, _dp, _ip, _ip, _ip, _ip]
+        L.orc_channel_create.restype = ct.c_void_p
+        L.orc_channel_create.argtypes = [ct.c_int, ct.c_int, ct.c_int, ct.c_double, ct.c_double, ct.c_double,
+                                         ct.c_double, ct.c_ulonglong, ct.c_int, _dp, ct.c_char_p, ct.c_int]
+        L.orc_eval_bc.restype = ct.c_int
+        L.orc_eval_bc.argtypes = [ct.c_void_p, _ip, _dp, _ip, _dp] + [_ip] * 4 + [_dp] * 4 + [ct.c_char_p, ct.c_int]
         L.orc_mesh_geometry.argtypes = [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
         L.orc_set_bc.argtypes = [ct.c_void_p, _ip, _ip, _ip, _ip, _dp, _dp, _dp, _dp]
         L.orc_lsq_gradient.argtypes = [ct.c_void_p, ct.c_int, _dp, _dp, _dp, _dp]
@@ -77,20 +85,62 @@ def _i(a):
 class Oracle:
     """Oracle mesh + boundary conditions; topology dict as returned by HostMesh.topology()."""
 
-    def __init__(self, topo: dict):
+    def __init__(self, topo: dict | None = None, _handle=None):
+        if _handle is None:
+            nf = len(topo["face_offsets"]) - 1
+            err = ct.create_string_buffer(1024)
+            h = lib().orc_mesh_create(len(topo["points"]) // 3, _d(topo["points"]), nf, _i(topo["face_offsets"]),
+                                      _i(topo["face_points"]), len(topo["neighbour"]), _i(topo["owner"]),
+                                      _i(topo["neighbour"]), len(topo["patch_start"]), _i(topo["patch_start"]),
+                                      _i(topo["patch_size"]), err, 1024)
+            if not h:
+                raise RuntimeError(err.value.decode())
+            _handle = h
+        self._h = ct.c_void_p(_handle)
+        s = np.zeros(6, np.int32)
+        lib().orc_mesh_sizes(self._h, _i(s))
+        self.n_points, self.n_faces, self.n_internal, self.n_cells, self.n_patches, self._nfp = map(int, s)
         self.t = topo
-        nf = len(topo["face_offsets"]) - 1
+
+    @classmethod
+    def channel(cls, nx, ny, nz, lx=2.5, ly=0.41, lz=0.41, jitter=0.0, seed=0, obstacle=False) -> "Oracle":
+        """The synthetic channel mesh built by the oracle itself (channel.cpp), hexes only."""
         err = ct.create_string_buffer(1024)
-        h = lib().orc_mesh_create(len(topo["points"]) // 3, _d(topo["points"]), nf, _i(topo["face_offsets"]),
-                                  _i(topo["face_points"]), len(topo["neighbour"]), _i(topo["owner"]),
-                                  _i(topo["neighbour"]), len(topo["patch_start"]), _i(topo["patch_start"]),
-                                  _i(topo["patch_size"]), err, 1024)
+        h = lib().orc_channel_create(nx, ny, nz, lx, ly, lz, jitter, seed, int(obstacle), None, err, 1024)
         if not h:
             raise RuntimeError(err.value.decode())
-        self._h = ct.c_void_p(h)
-        self.n_cells = lib().orc_mesh_ncells(self._h)
-        self.n_faces = nf
-        self.n_internal = len(topo["neighbour"])
+        return cls(_handle=h)
+
+    def topology(self) -> dict:
+        t = dict(points=np.zeros(3 * self.n_points), face_offsets=np.zeros(self.n_faces + 1, np.int32),
+                 face_points=np.zeros(self._nfp, np.int32), owner=np.zeros(self.n_faces, np.int32),
+                 neighbour=np.zeros(self.n_internal, np.int32), patch_start=np.zeros(self.n_patches, np.int32),
+                 patch_size=np.zeros(self.n_patches, np.int32))
+        lib().orc_mesh_topology(self._h, _d(t["points"]), _i(t["face_offsets"]), _i(t["face_points"]),
+                                _i(t["owner"]), _i(t["neighbour"]))
+        lib().orc_mesh_patches(self._h, _i(t["patch_start"]), _i(t["patch_size"]))
+        return t
+
+    def eval_bc(self, velocity: list, pressure: list) -> dict:
+        """Boundary values per patch (orc_eval_bc): velocity[k] = (ORC_VEL_* kind, params...),
+        pressure[k] = (ORC_P_* kind, value).  Returns the dict that set_bc takes."""
+        P, F = self.n_patches, self.n_faces
+        vk = np.array([v[0] for v in velocity], np.int32)
+        vp = np.zeros((P, 4))
+        for k, v in enumerate(velocity):
+            vp[k, :len(v) - 1] = v[1:]
+        pk = np.array([p[0] for p in pressure], np.int32)
+        pv = np.array([p[1] if len(p) > 1 else 0.0 for p in pressure], np.float64)
+        bc = {f"type_{q}": np.zeros(P, np.int32) for q in "uvwp"}
+        bc.update({q: np.zeros(F) for q in "uvwp"})
+        err = ct.create_string_buffer(1024)
+        vp = np.ascontiguousarray(vp.reshape(-1))
+        rc = lib().orc_eval_bc(self._h, _i(vk), _d(vp), _i(pk), _d(pv), _i(bc["type_u"]), _i(bc["type_v"]),
+                               _i(bc["type_w"]), _i(bc["type_p"]), _d(bc["u"]), _d(bc["v"]), _d(bc["w"]),
+                               _d(bc["p"]), err, 1024)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return bc
 
     def geometry(self) -> dict:
         C, F = self.n_cells, self.n_faces
@@ -185,6 +235,32 @@ class Oracle:
         if getattr(self, "_h", None) is not None and _lib is not None:
             _lib.orc_mesh_free(self._h)
             self._h = None
+
+
+VEL_WALL_NOSLIP, VEL_ZERO_GRADIENT, VEL_UNIFORM, VEL_PARABOLIC_BOX = 0, 1, 2, 3
+P_ZERO_GRADIENT, P_FIXED_VALUE = 0, 1
+
+
+def channel_case(nx, ny, nz, jitter=0.0, seed=0, obstacle=False, pout=0.0):
+    """The benchmark channel case built without the product library: the oracle's mesh, the
+    boundary values of the channel boundary file (patch_0_0 wall_noslip / zero_gradient p,
+    patch_1_0 parabolic_box_inlet 0.41 0.45 y z average_patch_normal / zero_gradient p, patch_2_0
+    zero_gradient / fixed_value pout, patch_3_0 wall_noslip / zero_gradient p) and the initial state
+    of main.cu:3302-3322 (mean inlet velocity everywhere, p = 0).  Returns (oracle, bc, state)."""
+    o = Oracle.channel(nx, ny, nz, jitter=jitter, seed=seed, obstacle=obstacle)
+    vel = [(VEL_WALL_NOSLIP,), (VEL_PARABOLIC_BOX, 0.41, 0.45, 1, 2), (VEL_ZERO_GRADIENT,)]
+    pre = [(P_ZERO_GRADIENT,), (P_ZERO_GRADIENT,), (P_FIXED_VALUE, pout)]
+    if obstacle:
+        vel.append((VEL_WALL_NOSLIP,))
+        pre.append((P_ZERO_GRADIENT,))
+    bc = o.eval_bc(vel, pre)
+    o.set_bc(bc)
+    t = o.topology()
+    sl = slice(int(t["patch_start"][1]), int(t["patch_start"][1] + t["patch_size"][1]))
+    C = o.n_cells
+    state = (np.full(C, bc["u"][sl].mean()), np.full(C, bc["v"][sl].mean()), np.full(C, bc["w"][sl].mean()),
+             np.zeros(C))
+    return o, bc, state
 
 
 def params(**kw) -> OrcParams:

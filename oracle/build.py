@@ -1,6 +1,7 @@
 """Builds the oracle (TEST INFRASTRUCTURE ONLY).
 
-  liboracle.so      oracle.cpp, the CPU restatement of the reference's SIMPLE iteration
+  liboracle.so      oracle.cpp, the CPU restatement of the reference's SIMPLE iteration, and
+                    channel.cpp, the synthetic channel case (mesh and boundary values)
   _ref/libgsv1ref.so the reference's own host code compiled from /root/reference where it lies
                      (only when that tree exists; see build_ref.sh for the recipe)
   _ref/libscalarref.so the reference's libpoisson / libscalar host assembly, same recipe
@@ -19,10 +20,11 @@ REFERENCE = Path("/root/reference")
 
 def build_oracle(force: bool = False) -> Path:
     out = HERE / "liboracle.so"
-    src = HERE / "oracle.cpp"
-    if force or not out.exists() or out.stat().st_mtime < max(src.stat().st_mtime, (HERE / "oracle.h").stat().st_mtime):
+    srcs = [HERE / "oracle.cpp", HERE / "channel.cpp"]
+    newest = max(p.stat().st_mtime for p in srcs + [HERE / "oracle.h"])
+    if force or not out.exists() or out.stat().st_mtime < newest:
         cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-o", str(out),
-               str(src)]
+               *map(str, srcs)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("oracle build failed:\n" + r.stderr)

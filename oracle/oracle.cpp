@@ -700,6 +700,41 @@ orc_mesh* orc_mesh_create(int nP, const double* pts, int nF, const int* fo, cons
 void orc_mesh_free(orc_mesh* m) { delete m; }
 int orc_mesh_ncells(const orc_mesh* m) { return m->nCells; }
 
+void orc_mesh_sizes(const orc_mesh* m, int* s) {
+  size_t nfp = 0;
+  for (const auto& f : m->faces) nfp += f.size();
+  s[0] = (int)m->P.size();
+  s[1] = m->nFaces;
+  s[2] = m->nInternal;
+  s[3] = m->nCells;
+  s[4] = (int)m->patchStart.size();
+  s[5] = (int)nfp;
+}
+
+void orc_mesh_patches(const orc_mesh* m, int* ps, int* pn) {
+  for (size_t k = 0; k < m->patchStart.size(); ++k) {
+    if (ps) ps[k] = m->patchStart[k];
+    if (pn) pn[k] = m->patchN[k];
+  }
+}
+
+void orc_mesh_topology(const orc_mesh* m, double* pts, int* fo, int* fp, int* own, int* nei) {
+  if (pts)
+    for (size_t i = 0; i < m->P.size(); ++i)
+      for (int q = 0; q < 3; ++q) pts[3 * i + q] = m->P[i][q];
+  int cur = 0;
+  for (int f = 0; f < m->nFaces; ++f) {
+    if (fo) fo[f] = cur;
+    for (int v : m->faces[f]) {
+      if (fp) fp[cur] = v;
+      ++cur;
+    }
+  }
+  if (fo) fo[m->nFaces] = cur;
+  if (own) std::copy(m->owner.begin(), m->owner.end(), own);
+  if (nei) std::copy(m->neigh.begin(), m->neigh.end(), nei);
+}
+
 void orc_mesh_geometry(const orc_mesh* m, double* cc, double* vol, double* xf, double* nf, double* sf, double* af,
                        double* mx) {
   for (int c = 0; c < m->nCells; ++c) {

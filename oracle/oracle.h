@@ -43,6 +43,31 @@ orc_mesh* orc_mesh_create(int n_points, const double* points, int n_faces, const
                           char* err, int errlen);
 void orc_mesh_free(orc_mesh* m);
 int orc_mesh_ncells(const orc_mesh* m);
+/* sizes: n_points, n_faces, n_internal, n_cells, n_patches, length of the face point list */
+void orc_mesh_sizes(const orc_mesh* m, int* s6);
+void orc_mesh_patches(const orc_mesh* m, int* patch_start, int* patch_size);
+/* topology back in the creation arrays' layout (any pointer may be NULL) */
+void orc_mesh_topology(const orc_mesh* m, double* points, int* face_off, int* face_pts, int* owner, int* neigh);
+
+/* Synthetic channel case (channel.cpp): Lx x Ly x Lz box of nx x ny x nz hexes, interior nodes
+ * jittered by +-jitter of the local spacing (mt19937_64(seed)), optionally without the obstacle
+ * block box = {x0, x1, y0, y1} (NULL: 0.45 0.55 0.15 0.25); patches patch_0_0 walls, patch_1_0
+ * inlet, patch_2_0 outlet, patch_3_0 obstacle. */
+orc_mesh* orc_channel_create(int nx, int ny, int nz, double Lx, double Ly, double Lz, double jitter,
+                             unsigned long long seed, int obstacle, const double* box, char* err, int errlen);
+
+/* Boundary values per patch (apply_bc_specs_to_legacy_face_arrays, velocity_bc_eval.cu:197-290):
+ * vkind per patch with 4 parameters each in vpar, pkind per patch with the fixed value in pval.
+ * Outputs as orc_set_bc takes them.  Returns 0, or 1 with a message in err. */
+#define ORC_VEL_WALL_NOSLIP 0
+#define ORC_VEL_ZERO_GRADIENT 1
+#define ORC_VEL_UNIFORM 2        /* vpar: ux uy uz */
+#define ORC_VEL_PARABOLIC_BOX 3  /* vpar: H Umax coordA coordB; average patch normal */
+#define ORC_P_ZERO_GRADIENT 0
+#define ORC_P_FIXED_VALUE 1
+int orc_eval_bc(const orc_mesh* m, const int* vkind, const double* vpar, const int* pkind, const double* pval,
+                int* tu, int* tv, int* tw, int* tp, double* uf, double* vf, double* wf, double* pf, char* err,
+                int errlen);
 void orc_mesh_geometry(const orc_mesh* m, double* cc, double* vol, double* xf, double* nf, double* sf,
                        double* af, double* max_nonorth);
 

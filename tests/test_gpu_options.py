@@ -1,0 +1,70 @@
+"""Reference options of the SIMPLE loop beyond the benchmark defaults, against the oracle.
+
+* nPressureCorr (main.cu:3521-3567): extra pressure passes b = -divCorr, dp' from zero,
+  p' += dp', flux correction again; run on the device (no host loops).
+* nVelNonOrthCorr (main.cu:3350-3384): momentum re-solves with the right-hand side re-assembled
+  on the current iterate until the relative change drops below corrTol; the relative change is a
+  device reduction.
+* pAmgSetupScope pressure (main.cu:2594-2598): the preconditioner is refreshed before every
+  pressure solve.  The fine matrix does not change within a step, so the fields equal those of the
+  per-step refresh bit for bit, whatever pAmgRebuildEvery says.
+"""
+import numpy as np
+import pytest
+
+import anabasis_b200 as anb
+import oracle
+from tests.cases import channel, initial_state, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(vel_tol=1e-15, p_tol=1e-15, vel_maxit=5000, p_maxit=20000)
+PRM = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3)
+MESH = dict(nx=24, ny=10, nz=10, jitter=0.15, seed=2, obstacle=True)
+
+
+def _run_both(steps, **opts):
+    m, bc, _ = channel(**MESH)
+    s = anb.Solver(m, anb.default_params(**PRM, **TIGHT, **opts))
+    s.set_bc(bc)
+    u0, v0, w0, p0 = initial_state(m, bc)
+    s.set_state(u0, v0, w0, p0)
+    rc, st = s.iterate(steps)
+    g = s.get_state()
+    o = oracle.Oracle(m.topology())
+    o.set_bc(bc)
+    oo = {k: v for k, v in opts.items() if k in ("n_pressure_corr", "n_vel_nonorth_corr", "corr_tol")}
+    ref, rst = o.run(oracle.params(**PRM, **TIGHT, **oo), steps, u0, v0, w0, p0)
+    return g, st, ref, rst
+
+
+@pytest.mark.parametrize("opts", [dict(n_pressure_corr=1), dict(n_pressure_corr=2, n_nonorth_corr=1),
+                                  dict(n_vel_nonorth_corr=2, corr_tol=1e-30),
+                                  dict(n_vel_nonorth_corr=3, corr_tol=1e-3, n_pressure_corr=1)])
+def test_options_against_oracle(opts):
+    g, st, ref, rst = _run_both(8, **opts)
+    assert len(st) == len(rst) == 8
+    for k in ("u", "v", "w", "p", "phi"):
+        assert rel_err(g[k], ref[k]) < 1e-8, (k, rel_err(g[k], ref[k]))
+    for a, b in zip(st, rst):
+        assert abs(a["du_rel"] - b["du"]) <= 1e-6 * b["du"] + 1e-14
+        assert abs(a["mass_res"] - b["mass_res"]) <= 1e-6 * max(b["mass_res"], 1e-13)
+
+
+def test_amg_setup_scope_pressure():
+    m, bc, _ = channel(**MESH)
+    out = []
+    for scope, every in ((0, 1), (1, 10)):
+        s = anb.Solver(m, anb.default_params(**PRM, p_amg_setup_scope=scope, p_amg_rebuild_every=every))
+        s.set_bc(bc)
+        s.set_state(*initial_state(m, bc))
+        s.iterate(6)
+        out.append(s.get_state())
+    for k in ("u", "v", "w", "p", "phi"):
+        assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_amg_setup_scope_rejects_unknown():
+    m, bc, _ = channel(6, 4, 4)
+    with pytest.raises(anb.AnbError):
+        anb.Solver(m, anb.default_params(**PRM, p_amg_setup_scope=2))
