@@ -123,6 +123,7 @@ SIGNATURES = {
     "anb_expand_case_args": (ct.c_int, [ct.c_int, ct.POINTER(ct.c_char_p), ct.c_char_p, ct.c_int, ct.c_char_p,
                                          ct.c_int]),
     "anb_write_vtu": (ct.c_int, [ct.c_void_p, ct.c_char_p, _dp, _dp, _dp, _dp, _dp, ct.c_char_p, ct.c_int]),
+    "anb_write_vtu_binary": (ct.c_int, [ct.c_void_p, ct.c_char_p, _dp, _dp, _dp, _dp, _dp, ct.c_char_p, ct.c_int]),
 }
 
 
@@ -224,11 +225,13 @@ class HostMesh:
             raise AnbError(ANB_ERR_INVALID, err.value.decode())
         return out
 
-    def write_vtu(self, filename, u, v, w, p, div_corr=None) -> None:
+    def write_vtu(self, filename, u, v, w, p, div_corr=None, binary=False) -> None:
+        """ASCII VTU as the reference writes it, or (binary=True) the appended raw-binary VTU."""
         err = ct.create_string_buffer(1024)
         dc = np.zeros(self.n_cells) if div_corr is None else np.ascontiguousarray(div_corr, np.float64)
         arrs = [np.ascontiguousarray(a, np.float64) for a in (u, v, w, p)]
-        if lib().anb_write_vtu(self._h, str(filename).encode(), *map(_d, arrs), _d(dc), err, 1024) != 0:
+        fn = lib().anb_write_vtu_binary if binary else lib().anb_write_vtu
+        if fn(self._h, str(filename).encode(), *map(_d, arrs), _d(dc), err, 1024) != 0:
             raise AnbError(ANB_ERR_IO, err.value.decode())
 
     def __del__(self):

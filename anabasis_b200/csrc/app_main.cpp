@@ -141,12 +141,14 @@ CylForce cylinder_forces(const HostMesh& m, int patch, const std::vector<double>
 
 void write_vtu_fields(const HostMesh& m, const std::string& fn, const std::vector<double>& u,
                       const std::vector<double>& v, const std::vector<double>& w, const std::vector<double>& p,
-                      const std::vector<double>& divCorr) {
+                      const std::vector<double>& divCorr, bool binary) {
   std::vector<double> umag(m.nCells);
   for (int c = 0; c < m.nCells; ++c) umag[c] = std::sqrt(u[c] * u[c] + v[c] * v[c] + w[c] * w[c]);
   const double* vec[3] = {u.data(), v.data(), w.data()};
-  write_vtu(m, fn, {"p", "umag", "cell_volume", "divCorr"}, {p.data(), umag.data(), m.vol.data(), divCorr.data()},
-            "U", vec);
+  const std::vector<std::string> names = {"p", "umag", "cell_volume", "divCorr"};
+  const std::vector<const double*> data = {p.data(), umag.data(), m.vol.data(), divCorr.data()};
+  if (binary) write_vtu_appended(m, fn, names, data, "U", vec);
+  else write_vtu(m, fn, names, data, "U", vec);
 }
 
 }  // namespace
@@ -375,7 +377,7 @@ int main(int argc, char** argv) {
       anb_get_state(ctx, u.data(), v.data(), w.data(), p.data(), nullptr);
       std::ostringstream oss;
       oss << par.outPrefix << "_iter" << std::setw(6) << std::setfill('0') << step << ".vtu";
-      write_vtu_fields(mesh, oss.str(), u, v, w, p, divCorr);
+      write_vtu_fields(mesh, oss.str(), u, v, w, p, divCorr, par.vtuBinary != 0);
     }
     if (!std::isfinite(st.mass_res) || st.mass_res > 1e50) {
       std::fprintf(stderr, "SIMPLE-like steady solve diverged.\n");
@@ -492,7 +494,7 @@ int main(int argc, char** argv) {
   if (par.write_vtu) {
     std::string vtu = par.outPrefix + "_final.vtu";
     try {
-      write_vtu_fields(mesh, vtu, u, v, w, p, divCorr);
+      write_vtu_fields(mesh, vtu, u, v, w, p, divCorr, par.vtuBinary != 0);
     } catch (const std::exception& e) {
       die(e.what());
     }

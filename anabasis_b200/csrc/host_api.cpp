@@ -214,4 +214,20 @@ int anb_write_vtu(anb_hmesh* h, const char* fn, const double* u, const double* v
   }
 }
 
+int anb_write_vtu_binary(anb_hmesh* h, const char* fn, const double* u, const double* v, const double* w,
+                         const double* p, const double* divCorr, char* eb, int el) {
+  try {
+    ensure_geom(h);
+    const auto& m = h->m;
+    std::vector<double> umag(m.nCells);
+    for (int c = 0; c < m.nCells; ++c) umag[c] = std::sqrt(u[c] * u[c] + v[c] * v[c] + w[c] * w[c]);
+    const double* vec[3] = {u, v, w};
+    anb::write_vtu_appended(m, fn, {"p", "umag", "cell_volume", "divCorr"}, {p, umag.data(), m.vol.data(), divCorr},
+                            "U", vec);
+    return 0;
+  } catch (const std::exception& e) {
+    return set_err(eb, el, e.what());
+  }
+}
+
 }  // extern "C"

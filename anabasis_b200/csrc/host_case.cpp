@@ -56,7 +56,7 @@ const std::map<std::string, std::string>& case_keys() {
       {"forceDragDir", "-force-drag-dir"}, {"forceLiftDir", "-force-lift-dir"},
       {"forceSpanDir", "-force-span-dir"}, {"forceUref", "-force-uref"}, {"forceAreaRef", "-force-area-ref"},
       {"profileSteps", "-profile-steps"}, {"assemblyBackend", "-assembly-backend"},
-      {"anbPrecision", "-anb-precision"}};
+      {"anbPrecision", "-anb-precision"}, {"anbVtuFormat", "-anb-vtu-format"}};
   return k;
 }
 
@@ -302,6 +302,12 @@ void parse_args(const std::vector<std::string>& a, Params& par) {
       if (v == "fp64" || v == "plain") par.precision = 0;
       else if (v == "mixed") par.precision = 1;
       else throw CliError("Unknown -anb-precision '" + v + "'. Use fp64 or mixed.", 1);
+    } else if (o == "-anb-vtu-format") {
+      need(o);
+      std::string v = a[++i];
+      if (v == "ascii") par.vtuBinary = 0;
+      else if (v == "binary" || v == "appended") par.vtuBinary = 1;
+      else throw CliError("Unknown -anb-vtu-format '" + v + "'. Use ascii or binary.", 1);
     }
   }
 }

@@ -35,6 +35,7 @@ struct Params {
   std::string wallPatchName = "patch_0_0", inletPatchName = "patch_1_0", outletPatchName = "patch_2_0";
   std::string bcConfigPath;
   int device = 0, velRestart = 40, velMaxit = 100, monitor = 1, write_vtu = 1;
+  int vtuBinary = 0;             // anbVtuFormat binary: appended raw VTU instead of the reference's ASCII
   int nVelNonOrthCorr = 0, nNonOrthCorr = 2, nPressureCorr = 0, nsteps = 1000, printEvery = 25, writeEvery = 0;
   double velTol = 1e-10, velRelTol = 0.0, corrTol = 1e-12, tolMass = 1e-10, tolVel = 1e-10;
   double uRelax = 0.7, pRelax = 1.0;

@@ -53,6 +53,13 @@ int anb_expand_case_args(int argc, const char* const* argv, char* out, int outle
 int anb_write_vtu(anb_hmesh* m, const char* filename, const double* u, const double* v, const double* w,
                   const double* p, const double* div_corr, char* errbuf, int errlen);
 
+/* The same VTU with every array as raw little-endian binary in one appended block
+ * (<AppendedData encoding="raw">, header_type UInt64): exact values, no text formatting.  No
+ * counterpart in the reference, whose writer is ASCII only (main.cu:975-983); the drop-in program
+ * selects it with the .case key anbVtuFormat binary. */
+int anb_write_vtu_binary(anb_hmesh* m, const char* filename, const double* u, const double* v, const double* w,
+                         const double* p, const double* div_corr, char* errbuf, int errlen);
+
 #ifdef __cplusplus
 }
 #endif
