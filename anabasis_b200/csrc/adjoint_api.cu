@@ -245,12 +245,11 @@ void mom_solve(anb_ctx* c, AdjointData& d, bool trans, const double* b, double* 
 
 // x (C) = A_p^{-1} b, from x = 0 (the caller scales b)
 void p_solve(anb_ctx* c, AdjointData& d, const double* b, double* x) {
-  PcgArgs a = pcg_args(c, b, x, d.pRtol);
+  PcgArgs a = pcg_args(c, b, d.pRtol);
   a.atol = 0.0;
   a.maxit = 500;
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
-  if (amg) c->amg.lv[0].b = c->pr;
-  CK(cudaMemsetAsync(x, 0, sizeof(double) * c->C, c->stream));
+  CK(cudaMemsetAsync(a.x, 0, sizeof(double) * c->C, c->stream));
   pcg_init(c->lc, a);
   pcg_precondition(c->lc, a, amg);
   int it = 0;
@@ -259,6 +258,7 @@ void p_solve(anb_ctx* c, AdjointData& d, const double* b, double* x) {
     poll(c, a.fl, 4);
     if (c->hFlags[0] || it > a.maxit) break;
   }
+  CK(cudaMemcpyAsync(x, a.x, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
   d.pIts += c->hFlags[1];
 }
 

@@ -171,12 +171,15 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
 
 void ensure_amg(anb_ctx* c);
 
-PcgArgs pcg_args(anb_ctx* c, const double* b, double* x, double rtol) {
+// FP64 PCG arguments; the iterate is the context's fixed work vector pxw (copy the caller's x in
+// before pcg_init and out after the solve).
+PcgArgs pcg_args(anb_ctx* c, const double* b, double rtol) {
   PcgArgs a{};
   a.A = p_sell(c);
   a.b = b;
-  a.x = x;
+  a.x = c->pxw;
   a.r = c->pr; a.z = c->pz; a.p0 = c->pp0; a.p1 = c->pp1; a.q = c->pq;
+  a.r2 = c->pr2;
   a.sc = c->scal + kScalPcg;
   a.fl = c->flags + kFlagPcg;
   a.atol = c->prm.p_tol;
@@ -190,9 +193,9 @@ PcgArgs pcg_args(anb_ctx* c, const double* b, double* x, double rtol) {
 void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
   ProfScope whole(c->lc, kKfPressureSolve, 0.0, 0);
   if (c->mixed) return solve_pressure_mixed(c, b, x, rtol, its, conv);
-  PcgArgs a = pcg_args(c, b, x, rtol);
+  PcgArgs a = pcg_args(c, b, rtol);
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
-  if (amg) c->amg.lv[0].b = c->pr;
+  CK(cudaMemcpyAsync(c->pxw, x, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
   pcg_init(c->lc, a);
   pcg_precondition(c->lc, a, amg);
   // enqueue most of the expected iterations (previous solve's count) before the first poll,
@@ -206,6 +209,7 @@ void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* it
     if (c->hFlags[0] || it > a.maxit + 2) break;
     batch = tail;
   }
+  CK(cudaMemcpyAsync(x, c->pxw, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
   *its = c->hFlags[1];
   *conv = c->hFlags[2] != 0;
   c->lastPIts = std::max(1, *its);
@@ -221,6 +225,7 @@ PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, do
   a.b = b;
   a.x = x;
   a.r = c->pr32; a.z = c->pz32; a.p0 = c->pp0_32; a.p1 = c->pp1_32; a.q = c->pq32;
+  a.r2 = c->pr2_32;
   a.sc = c->scal + kScalPcg;
   a.fl = c->flags + kFlagPcg;
   a.atol = atol;
@@ -292,6 +297,12 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
     d.x2 = ar.alloc<T>(h.n);
     if (l + 1 < A.nLevels) {
       d.agg = ar.upload(h.agg);
+      if (l == 0 || !h.sliceOff.empty()) {  // SELL level: the aggregate of every slot's column
+        const std::vector<int>& col = l == 0 ? c->L.col : h.col;
+        std::vector<int> sa(col.size());
+        for (size_t e = 0; e < col.size(); ++e) sa[e] = h.agg[col[e]];
+        d.slotAgg = ar.upload(sa);
+      }
       d.memOff = ar.upload(h.memOff);
       d.mem = ar.upload(h.mem);
       d.gOff = ar.upload(h.gOff);
@@ -315,10 +326,7 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
     std::fprintf(stderr, " | tail rows %d, cluster %d\n", A.tailRows, A.tailCluster);
   }
   const char* noGraph = std::getenv("ANB_NO_GRAPH");
-  if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) {
-    A.lv[0].b = ga.r;
-    CK(amg_capture_graph(c->lc, ga, A));
-  }
+  if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) CK(amg_capture_graph(c->lc, ga, A));
 }
 
 void ensure_amg(anb_ctx* c) {
@@ -329,7 +337,7 @@ void ensure_amg(anb_ctx* c) {
     if (c->amg32.nLevels >= 2) amg_refresh(c->lc, c->amg32);
     return;
   }
-  if (!c->amgBuilt) build_amg<double>(c, c->amg, c->pval, c->pdiag, c->pwdinv, pcg_args(c, c->pb, c->Pc, 0.0));
+  if (!c->amgBuilt) build_amg<double>(c, c->amg, c->pval, c->pdiag, c->pwdinv, pcg_args(c, c->pb, 0.0));
   if (c->amg.nLevels >= 2) amg_refresh(c->lc, c->amg);
 }
 
@@ -434,7 +442,6 @@ void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, i
   d.rtol = rtol;
   d.red = c->red;
   const AmgDevT<float>* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg32.nLevels >= 2) ? &c->amg32 : nullptr;
-  if (amg) c->amg32.lv[0].b = c->pr32;
   int tot = 0;
   bool ok = false;
   for (int sweep = 0;; ++sweep) {
@@ -688,13 +695,17 @@ void build_slot_lookup(anb_ctx* c) {
 
 void release_amg(anb_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
-  if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
-  c->amg.graph = nullptr;
+  for (auto& g : c->amg.graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
   c->amg.graphKernels = 0;
   c->amg.nLevels = 0;
   c->amg.dense = nullptr;
-  if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
-  c->amg32.graph = nullptr;
+  for (auto& g : c->amg32.graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
   c->amg32.graphKernels = 0;
   c->amg32.nLevels = 0;
   c->amg32.dense = nullptr;
@@ -896,6 +907,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       c->pp0_32 = A.alloc<float>(C);
       c->pp1_32 = A.alloc<float>(C);
       c->pq32 = A.alloc<float>(C);
+      c->pr2_32 = A.alloc<float>(C);
       CK(cudaMemset(c->mval32, 0, sizeof(float) * c->nEnt));
       CK(cudaMemset(c->pval32, 0, sizeof(float) * c->nEnt));
       CK(cudaMemset(c->dx32, 0, sizeof(float) * 3 * C));
@@ -914,6 +926,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       c->pp0 = A.alloc<double>(C);
       c->pp1 = A.alloc<double>(C);
       c->pq = A.alloc<double>(C);
+      c->pr2 = A.alloc<double>(C);
+      c->pxw = A.alloc<double>(C);
       c->pwdinv = A.alloc<double>(C);
     }
     c->pdx = A.alloc<double>(C);
@@ -959,8 +973,10 @@ void anb_destroy(anb_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->prm.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->amg.graph) cudaGraphExecDestroy(c->amg.graph);
-  if (c->amg32.graph) cudaGraphExecDestroy(c->amg32.graph);
+  for (auto g : c->amg.graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto g : c->amg32.graph)
+    if (g) cudaGraphExecDestroy(g);
   adjoint_release(c);
   c->amgArena.release();
   c->arena.release();

@@ -95,6 +95,9 @@ struct anb_ctx {
   double* UsPrev = nullptr;   // momentum iterates before a re-solve (3*C; only with nVelNonOrthCorr > 0)
   double *bw[8] = {nullptr};  // BiCGSTAB work vectors (3*C each)
   double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pq = nullptr, *pdx = nullptr;
+  // second PCG residual buffer and the PCG iterate at a fixed address (the captured V-cycles update
+  // both in place); solve_pressure copies the caller's x in and out
+  double *pr2 = nullptr, *pxw = nullptr;
   double* pwdinv = nullptr;   // omega / pressure diagonal (level-0 smoother)
   double* scal = nullptr;     // device scalars
   int* flags = nullptr;
@@ -121,7 +124,7 @@ struct anb_ctx {
   float *mval32 = nullptr, *mdiag32 = nullptr, *pval32 = nullptr, *pdiag32 = nullptr, *pwdinv32 = nullptr;
   float* bw32[8] = {nullptr};
   float *r32 = nullptr, *dx32 = nullptr;                     // 3*nCells each
-  float *pr32 = nullptr, *pz32 = nullptr, *pp0_32 = nullptr, *pp1_32 = nullptr, *pq32 = nullptr;
+  float *pr32 = nullptr, *pz32 = nullptr, *pp0_32 = nullptr, *pp1_32 = nullptr, *pq32 = nullptr, *pr2_32 = nullptr;
   AmgDevT<float> amg32;
   double innerRtol = 1e-4;    // relative reduction asked of one FP32 inner solve at most
   // scalar-library solves (allocated on first use)
@@ -165,7 +168,7 @@ DSell p_sell(const anb_ctx* c);
 void grad(anb_ctx* c, int nf, const double* const* phi, const unsigned char* bits, double* const* out);
 void poll(anb_ctx* c, const int* dflags, int count);
 void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]);
-PcgArgs pcg_args(anb_ctx* c, const double* b, double* x, double rtol);
+PcgArgs pcg_args(anb_ctx* c, const double* b, double rtol);
 void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv);
 void ensure_amg(anb_ctx* c);
 void launch_mom(anb_ctx* c, const double* Q, int rhsOnly);

@@ -233,6 +233,10 @@ struct PcgArgsT {
   const T* b;
   T* x;
   T *r, *z, *p0, *p1, *q;
+  // AMG-preconditioned iterations keep the residual in two buffers (r, r2): the V-cycle's level-0
+  // down sweep applies r_new = r - alpha q and x += alpha p itself, reading the old residual of
+  // the neighbour rows from one buffer while it writes the new one into the other.
+  T* r2;
   double* sc;         // rz, alpha, beta, eps, rr, pq
   int* fl;            // done, iters, converged, first
   double atol, rtol;
@@ -258,6 +262,7 @@ struct AmgLevelDevT {
   const int* mem;
   const int* gOff;     // Galerkin gather for the next level's storage
   const int* gIdx;
+  const int* slotAgg;  // SELL levels: aggregate of each storage slot's column, agg[col[e]]
   int nEntNext;        // next level's SELL storage entries
   // work vectors
   T *b, *x, *x2;
@@ -276,7 +281,9 @@ struct AmgDevT {
   // iterations on the jittered obstacle channel (105 -> 66 per outer step at 970k cells).
   double omega = 0.9;
   double corr = 1.6;
-  cudaGraphExec_t graph = nullptr;  // captured V-cycle (see amg_capture_graph)
+  // captured V-cycles (see amg_capture_graph): variant v reads the residual buffer v (r, r2) and
+  // writes the other one, with the search direction p0 (v = 0) or p1 (v = 1)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graphKernels = 0;
   // Coarse tail: the CSR levels with at most tailRows rows and the dense level run as one
   // thread-block-cluster kernel of tailCluster CTAs (0: one launch per level and sweep).

@@ -34,13 +34,12 @@ __device__ __forceinline__ int slot_regs(const DMesh& m, int r, int (&f)[WM], in
 
 // ---- least-squares gradient: main.cu:1403-1440 on the moments of main.cu:1159-1251 ----------
 template <int NF>
-__device__ __forceinline__ void grad_slot(const DMesh& m, const GradArgs& a, int r, int e, int c,
+__device__ __forceinline__ void grad_slot(const DMesh& m, const GradArgs& a, int c, const double (&ccr)[3],
                                           const double (&pr)[NF], double (&b)[NF][3]) {
-  // cc_c - cc_r: the slot's d (cc_N - cc_P) with the sign of the row's side, bit for bit
-  const double sgn = r < c ? 1.0 : -1.0;
-  const size_t n = (size_t)m.nEnt;
-  const double r0 = sgn * __ldg(&m.slotGeom[5 * n + e]), r1 = sgn * __ldg(&m.slotGeom[6 * n + e]),
-               r2 = sgn * __ldg(&m.slotGeom[7 * n + e]);
+  // r = cc_c - cc_r from the cell centres (neighbour centres are L2-resident gathers): for the
+  // owner row this is the face's d = cc_N - cc_P, for the neighbour row its negation, bit for bit
+  const double r0 = __ldg(&m.cc[3 * c]) - ccr[0], r1 = __ldg(&m.cc[3 * c + 1]) - ccr[1],
+               r2 = __ldg(&m.cc[3 * c + 2]) - ccr[2];
   const double w = 1.0 / fmax(r0 * r0 + r1 * r1 + r2 * r2, 1e-30);
 #pragma unroll
   for (int f = 0; f < NF; ++f) {
@@ -61,19 +60,20 @@ __global__ void __launch_bounds__(kBlock) k_lsq_grad(DMesh m, GradArgs a) {
       pr[f] = __ldg(&a.phi[f][r]);
       b[f][0] = b[f][1] = b[f][2] = 0.0;
     }
+    const double ccr[3] = {__ldg(&m.cc[3 * r]), __ldg(&m.cc[3 * r + 1]), __ldg(&m.cc[3 * r + 2])};
     if constexpr (WM > 0) {
       int fs[WM], cs[WM];
-      const int base = slot_regs<WM>(m, r, fs, cs);
+      slot_regs<WM>(m, r, fs, cs);
 #pragma unroll
       for (int k = 0; k < WM; ++k)
-        if (fs[k] >= 0) grad_slot<NF>(m, a, r, base + (k << 5), cs[k], pr, b);
+        if (fs[k] >= 0) grad_slot<NF>(m, a, cs[k], ccr, pr, b);
     } else {
       int W;
       const int base = row_base(m, r, W);
       for (int k = 0; k < W; ++k) {
         const int e = base + (k << 5);
         if (__ldg(&m.slotFace[e]) < 0) break;
-        grad_slot<NF>(m, a, r, e, __ldg(&m.col[e]), pr, b);
+        grad_slot<NF>(m, a, __ldg(&m.col[e]), ccr, pr, b);
       }
     }
     const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);

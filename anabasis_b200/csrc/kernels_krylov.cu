@@ -425,6 +425,20 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld,
   }
 }
 
+// Iteration count and convergence test on |r|^2 = rr (last block, thread 0).
+template <class T>
+__device__ __forceinline__ void pcg_converged(const PcgArgsT<T>& a, double rr) {
+  a.sc[4] = rr;
+  a.fl[1] += 1;
+  if (sqrt(rr) <= a.sc[3]) {
+    a.fl[0] = 1;
+    a.fl[2] = 1;
+  } else if (a.fl[1] >= a.maxit || a.sc[5] == 0.0) {
+    a.fl[0] = 1;
+    a.fl[2] = 0;
+  }
+}
+
 // x += alpha p ; r -= alpha q ; convergence test on |r|
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgsT<T> a, const T* p) {
@@ -434,22 +448,12 @@ __global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgsT<T> a, const T* p) {
   const double al = a.sc[1];
   double acc[1] = {0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    a.x[r] = (T)((double)a.x[r] + al * (double)p[r]);
-    const double rr = (double)a.r[r] - al * (double)a.q[r];
+    a.x[r] = (T)__fma_rn(al, (double)p[r], (double)a.x[r]);
+    const double rr = __fma_rn(-al, (double)a.q[r], (double)a.r[r]);
     a.r[r] = (T)rr;
     acc[0] += rr * rr;
   }
-  if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    a.sc[4] = acc[0];
-    a.fl[1] += 1;
-    if (sqrt(acc[0]) <= a.sc[3]) {
-      a.fl[0] = 1;
-      a.fl[2] = 1;
-    } else if (a.fl[1] >= a.maxit || a.sc[5] == 0.0) {
-      a.fl[0] = 1;
-      a.fl[2] = 0;
-    }
-  }
+  if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) pcg_converged(a, acc[0]);
 }
 
 // ---------------------------------------------------------------- AMG V-cycle
@@ -484,6 +488,63 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
     f.x[i] = (T)xi;
     f.x2[i] = (T)(bi - ax);
   }
+}
+
+// Level-0 down sweep fused with the update of the PCG iteration before it: r_new = r - alpha q and
+// x += alpha p on the row's own entries, |r_new|^2 with the convergence test in the last block,
+// then the pre-smoothing x0 = w D^-1 r_new and the residual x2 = r_new - A x0.  The neighbours'
+// r_new come from their old residual and q, rounded to T as their own rows store them, so the
+// values are those of a separate update kernel followed by k_amg_resid.  The old residual is read
+// from rIn and the new one written to rOut (other rows still read rIn).  Right after pcg_init
+// (flag "first") there is no update: r_new = r.
+template <class T, int WM>
+__global__ void __launch_bounds__(kBlock) k_amg_resid0(PcgArgsT<T> a, AmgLevelDevT<T> f, const T* rIn, T* rOut,
+                                                       const T* p) {
+  __shared__ double sm[32];
+  if (a.fl[0]) return;
+  const bool upd = a.fl[3] == 0;
+  const double al = upd ? a.sc[1] : 0.0;
+  double acc[1] = {0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
+    double ri;
+    if (upd) {
+      const double rr = __fma_rn(-al, ld(&a.q[i]), ld(&rIn[i]));
+      acc[0] += rr * rr;
+      ri = (double)(T)rr;
+      a.x[i] = (T)__fma_rn(al, (double)p[i], (double)a.x[i]);
+    } else {
+      ri = ld(&rIn[i]);
+    }
+    rOut[i] = (T)ri;
+    const double di = ld(&f.diag[i]);
+    const double xi = ld(&f.wdinv[i]) * ri;
+    double ax = di * xi;
+    if constexpr (WM == 0) {
+      const int s = i >> 5;
+      const int b = __ldg(&f.sliceOff[s]) + (i & 31);
+      const int W = (__ldg(&f.sliceOff[s + 1]) - __ldg(&f.sliceOff[s])) >> 5;
+#pragma unroll 4
+      for (int k = 0; k < W; ++k) {
+        const int e = b + (k << 5);
+        const int j = __ldg(&f.col[e]);
+        const double rj = upd ? (double)(T)__fma_rn(-al, ld(&a.q[j]), ld(&rIn[j])) : ld(&rIn[j]);
+        ax += ld(&f.val[e]) * (ld(&f.wdinv[j]) * rj);
+      }
+    } else {
+      int c[WM];
+      double v[WM];
+      sell_regs<WM>(f.sliceOff, f.col, f.val, i, c, v);
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        const double rj = upd ? (double)(T)__fma_rn(-al, ld(&a.q[c[k]]), ld(&rIn[c[k]])) : ld(&rIn[c[k]]);
+        ax += v[k] * (ld(&f.wdinv[c[k]]) * rj);
+      }
+    }
+    f.x[i] = (T)xi;
+    f.x2[i] = (T)(ri - ax);
+  }
+  if (!upd) return;  // uniform over the grid
+  if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) pcg_converged(a, acc[0]);
 }
 
 constexpr int kCoarseLanes = 8;  // lanes per row on the CSR coarse levels
@@ -678,15 +739,29 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
       for (int k = 0; k < W; ++k) {
         const int ee = b + (k << 5);
         const int j = __ldg(&f.col[ee]);
-        ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
+        ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.slotAgg[ee])]));
       }
     } else {
-      int c[WM];
+      // column, value and the column's aggregate of every slot first (no col -> agg load chain);
+      // slots past the row's width read as (row i, value 0, aggregate of row i)
+      const int s = i >> 5;
+      const int b0 = __ldg(&f.sliceOff[s]);
+      const int W = (__ldg(&f.sliceOff[s + 1]) - b0) >> 5;
+      const int base = b0 + (i & 31);
+      const int gi = __ldg(&f.agg[i]);
+      int c[WM], g[WM];
       double v[WM];
-      sell_regs<WM>(f.sliceOff, f.col, f.val, i, c, v);
-      int g[WM];
 #pragma unroll
-      for (int k = 0; k < WM; ++k) g[k] = __ldg(&f.agg[c[k]]);
+      for (int k = 0; k < WM; ++k) {
+        c[k] = i;
+        g[k] = gi;
+        v[k] = 0.0;
+        if (k < W) {
+          c[k] = __ldg(&f.col[base + (k << 5)]);
+          g[k] = __ldg(&f.slotAgg[base + (k << 5)]);
+          v[k] = ld(&f.val[base + (k << 5)]);
+        }
+      }
 #pragma unroll
       for (int k = 0; k < WM; ++k) ax += v[k] * (ld(&f.x[c[k]]) + corr * ld(&e[g[k]]));
     }
@@ -1022,18 +1097,25 @@ void amg_configure_tail(AmgDevT<T>& amg, int tailRows, cudaStream_t s) {
   }
 }
 
+// One V-cycle z = M^-1 r_new, fused at level 0 with the PCG update r_new = r - alpha q,
+// x += alpha p (see k_amg_resid0): variant v reads the residual buffer v (0: a.r, 1: a.r2), writes
+// the other and updates x with p_v.
 template <class T>
-static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
+static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg, int v) {
   const int L = amg->nLevels;
-  // level 0 right-hand side is the PCG residual
+  const T* rIn = v ? a.r2 : a.r;
+  T* rOut = v ? a.r : a.r2;
+  const T* p = v ? a.p1 : a.p0;
+  AmgLevelDevT<T> f0 = amg->lv[0];
+  f0.b = rOut;  // level 0 right-hand side is the new PCG residual
   {
-    const AmgLevelDevT<T>& f = amg->lv[0];
+    const AmgLevelDevT<T>& f = f0;
     ProfScope ps(lc, kKfAmgResid0, 0.0, 2);
     const int wc = sell_width_class(f.maxW);
     const int nb = blocks_for(f.n, lc.rowBlocks);
-    if (wc == 4) k_amg_resid<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
-    else if (wc == 8) k_amg_resid<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
-    else k_amg_resid<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+    if (wc == 4) k_amg_resid0<T, 4><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
+    else if (wc == 8) k_amg_resid0<T, 8><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
+    else k_amg_resid0<T, 0><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
@@ -1085,7 +1167,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     }
   }
   {
-    const AmgLevelDevT<T>& f = amg->lv[0];
+    const AmgLevelDevT<T>& f = f0;
     const T* e = (L == 2) ? amg->lv[1].x : amg->lv[1].x2;
     ProfScope ps(lc, kKfAmgUp0, 0.0);
     const int wc = sell_width_class(f.maxW);
@@ -1096,48 +1178,62 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
   }
 }
 
+// V-cycle variant v (graph when captured)
+template <class T>
+static void apply_vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg, int v) {
+  if (amg->graph[v]) {
+    g_launches += amg->graphKernels;
+    cudaGraphLaunch(amg->graph[v], lc.stream);
+  } else {
+    vcycle(lc, a, amg, v);
+  }
+}
+
 template <class T>
 void pcg_precondition(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
   if (!amg || amg->nLevels < 2) {
     g_launches += 1;
     k_pcg_jacobi<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-  } else if (amg->graph) {
-    g_launches += amg->graphKernels;
-    cudaGraphLaunch(amg->graph, lc.stream);
   } else {
-    vcycle(lc, a, amg);
+    apply_vcycle(lc, a, amg, 0);  // right after pcg_init: no update, r copied to r2
   }
 }
 
-// Records one V-cycle into a CUDA graph.  Every pointer and scalar the V-cycle kernels read is
-// fixed for the life of the hierarchy (values change on refresh, addresses do not), so the
-// graph is captured once and replayed for every preconditioner application.
+// Records the two V-cycle variants into CUDA graphs.  Every pointer and scalar the V-cycle kernels
+// read is fixed for the life of the hierarchy (values change on refresh, addresses do not; the
+// callers keep x, r, r2, p0, p1, q and z at fixed addresses), so the graphs are captured once and
+// replayed for every preconditioner application.
 template <class T>
 cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
-  if (amg.graph) {
-    cudaGraphExecDestroy(amg.graph);
-    amg.graph = nullptr;
-  }
+  for (int v = 0; v < 2; ++v)
+    if (amg.graph[v]) {
+      cudaGraphExecDestroy(amg.graph[v]);
+      amg.graph[v] = nullptr;
+    }
   LaunchCfg quiet = lc;
   quiet.prof = nullptr;
-  const long long before = g_launches.load();
-  cudaGraph_t g = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(lc.stream, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) return e;
-  vcycle(quiet, a, &amg);
-  e = cudaStreamEndCapture(lc.stream, &g);
-  amg.graphKernels = (int)(g_launches.load() - before);
-  g_launches -= amg.graphKernels;
-  if (e != cudaSuccess) return e;
-  e = cudaGraphInstantiate(&amg.graph, g, 0);
-  cudaGraphDestroy(g);
-  return e;
+  for (int v = 0; v < 2; ++v) {
+    const long long before = g_launches.load();
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(lc.stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    vcycle(quiet, a, &amg, v);
+    e = cudaStreamEndCapture(lc.stream, &g);
+    amg.graphKernels = (int)(g_launches.load() - before);
+    g_launches -= amg.graphKernels;
+    if (e != cudaSuccess) return e;
+    e = cudaGraphInstantiate(&amg.graph[v], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 template <class T>
 void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgDevT<T>* amg) {
   const T* pOld = (it & 1) ? a.p1 : a.p0;
   T* pNew = (it & 1) ? a.p0 : a.p1;
+  const bool useAmg = amg && amg->nLevels >= 2;
   {
     // algorithmic bytes: 12 B per off-diagonal (value + column) and 40 B per row in FP64;
     // values and vectors halve in FP32
@@ -1147,6 +1243,12 @@ void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgD
     if (wc == 4) k_pcg_pq<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
     else if (wc == 8) k_pcg_pq<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
     else k_pcg_pq<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+  }
+  if (useAmg) {
+    // the V-cycle's level-0 sweep applies x += alpha pNew, r -= alpha q: variant (it + 1) & 1 reads
+    // the residual this iteration starts from and uses pNew (p1 on even iterations)
+    apply_vcycle(lc, a, amg, (it + 1) & 1);
+    return;
   }
   {
     ProfScope ps(lc, kKfPcgUpdate, 0.0);

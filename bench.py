@@ -306,6 +306,35 @@ def run_reference(args, rank: int, world: int) -> dict | None:
     }
 
 
+def run_cpu_baselines(args) -> dict:
+    """The oracle port (C++/OpenMP, all host threads, Jacobi-PCG / Jacobi-BiCGSTAB at the reference's
+    1e-10 tolerances) on configurations 1-3, each case built by the oracle alone: config 1 (16,000
+    hexes) for 300 steps from the initial state, config 2 (970,480 cells) and config 3 (3,977,792
+    cells) on bounded samples of steps 1..k.  No product library is loaded."""
+    import oracle
+
+    nthreads = os.cpu_count() or 1
+    rows = []
+    for name, kw, steps in (("config 1: channel 40x20x20 (16000 hex)", dict(nx=40, ny=20, nz=20), 300),
+                            ("config 2: obstacle channel 200x70x70 jittered (seed 0)", WORKLOAD, 3),
+                            ("config 3: obstacle channel 320x112x112 jittered (seed 1)",
+                             dict(nx=320, ny=112, nz=112, jitter=0.15, seed=1, obstacle=True), 2)):
+        t0 = time.perf_counter()
+        o, bc, state = oracle.channel_case(**kw)
+        setup = time.perf_counter() - t0
+        prm = oracle.params(n_threads=nthreads, tol_mass=0.0, tol_vel=0.0, **PARAMS)
+        t0 = time.perf_counter()
+        _, st = o.run(prm, steps, *state)
+        dt = time.perf_counter() - t0
+        rows.append({"case": name, "cells": o.n_cells, "steps": len(st), "seconds": dt,
+                     "cell_iters_per_s": o.n_cells * len(st) / dt, "ms_per_step": 1e3 * dt / len(st),
+                     "setup_s": setup, "mass_res_last": st[-1]["mass_res"],
+                     "pcg_its_last_step": st[-1]["its_p_total"]})
+        del o
+    return {"metric": "SIMPLE cell-iters/s, CPU oracle port", "unit": "cell-iters/s", "cores": nthreads,
+            "kind": "port", "data": "synthetic", "rows": rows}
+
+
 def _peak_device_bytes(device: int = 0) -> int | None:
     """Device memory in use (NVML, read-only query).  The library allocates every buffer of a
     phase up front and keeps it until the context is destroyed, so the figure taken at the end of
@@ -485,7 +514,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--config", default="obstacle1m", choices=["obstacle1m", "mixed4m", "adjoint1m", "tets16m"],
+    ap.add_argument("--config", default="obstacle1m",
+                    choices=["obstacle1m", "mixed4m", "adjoint1m", "tets16m", "cpu3"],
                     help="obstacle1m: the headline SIMPLE throughput line; the others are single-GPU studies "
                          "of the mixed-precision, adjoint and 16M-tet configurations")
     ap.add_argument("--max-steps", type=int, default=4000)
@@ -498,7 +528,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    studies = {"mixed4m": run_mixed4m, "adjoint1m": run_adjoint1m, "tets16m": run_tets16m}
+    studies = {"mixed4m": run_mixed4m, "adjoint1m": run_adjoint1m, "tets16m": run_tets16m,
+               "cpu3": run_cpu_baselines}
     if args.impl == "reference":
         out = run_reference(args, rank, world)
     elif args.config in studies:
