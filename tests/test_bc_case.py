@@ -102,6 +102,27 @@ def test_reference_bc_configs(mesh, bc):
 
 
 @needs_ref
+def test_fixed_flow_rate_planarity_check(mesh, tmp_path):
+    # velocity_bc_eval.cu:122-134: a flow rate along the average normal of a patch that is not
+    # planar (the four channel walls: the area vectors cancel) is rejected with the same message
+    f = tmp_path / "nonplanar.bc"
+    f.write_text(BC_FILES["parabolic"].replace("velocity patch_0_0 wall_noslip",
+                                               "velocity patch_0_0 fixed_flow_rate 1e-3 average_patch_normal"))
+    with pytest.raises(anb.AnbError) as mine:
+        anb.HostMesh.read(mesh).evaluate_bc(f)
+    with pytest.raises(RuntimeError) as ref:
+        refshim.RefMesh(mesh).bc_eval(f)
+    assert "planarity" in str(ref.value)
+    assert str(ref.value) in str(mine.value)
+    # the same flow rate along the local face normals is accepted by both, with equal values
+    f.write_text(BC_FILES["parabolic"].replace("velocity patch_0_0 wall_noslip",
+                                               "velocity patch_0_0 fixed_flow_rate 1e-3 local_face_normal"))
+    a, b = anb.HostMesh.read(mesh).evaluate_bc(f), refshim.RefMesh(mesh).bc_eval(f)
+    for k in ("u", "v", "w", "type_u"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+@needs_ref
 @pytest.mark.parametrize("line", BAD_LINES)
 def test_bc_errors_same_message(mesh, tmp_path, line):
     f = tmp_path / "bad.bc"
