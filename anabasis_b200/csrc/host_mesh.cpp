@@ -45,37 +45,62 @@ std::string read_file(const std::string& fn) {
   return s;
 }
 
-// Removes /* */ blocks (an unterminated one stays) and // line comments, main.cu:533-537.
+// Removes /* */ blocks (an unterminated one stays) and // line comments, main.cu:533-537, in one
+// linear pass each.  The reference erases the first "/*" ... "*/" block and searches the edited
+// string again from its start, so a '/' just before an erased block and a '*' just after it form a
+// new block start; the scan below reproduces that.
 std::string strip_comments(const std::string& txt) {
+  const size_t npos = std::string::npos;
   std::string s;
   s.reserve(txt.size());
-  size_t i = 0, n = txt.size();
-  bool blocks = true;
-  while (i < n) {
-    if (blocks && txt[i] == '/' && i + 1 < n && txt[i + 1] == '*') {
-      size_t e = txt.find("*/", i + 2);
-      if (e == std::string::npos) {
-        blocks = false;
-        continue;
-      }
-      i = e + 2;
-      continue;
+  size_t i = 0;
+  while (true) {
+    const size_t a = txt.find("/*", i);
+    if (a == npos) {
+      s.append(txt, i, npos);
+      break;
     }
-    s.push_back(txt[i]);
-    ++i;
+    const size_t b = txt.find("*/", a + 2);
+    if (b == npos) {  // unterminated: the rest stays as it is
+      s.append(txt, i, npos);
+      break;
+    }
+    s.append(txt, i, a - i);
+    i = b + 2;
+    // a '/' left before the erased block and a '*' after it make the next block start
+    bool stop = false;
+    while (!s.empty() && s.back() == '/' && i < txt.size() && txt[i] == '*') {
+      const size_t e = txt.find("*/", i + 1);
+      if (e == npos) {  // unterminated: the reference stops erasing here, the rest stays
+        s.append(txt, i, npos);
+        stop = true;
+        break;
+      }
+      s.pop_back();
+      i = e + 2;
+    }
+    if (stop) break;
   }
   std::string out;
   out.reserve(s.size() + 1);
+  const char* base = s.data();
+  const size_t n = s.size();
   size_t a = 0;
-  while (a < s.size()) {
-    size_t e = s.find('\n', a);
-    size_t lineEnd = (e == std::string::npos) ? s.size() : e;
-    size_t c = s.find("//", a);
-    size_t cut = (c != std::string::npos && c < lineEnd) ? c : lineEnd;
+  while (a < n) {
+    const char* nl = static_cast<const char*>(std::memchr(base + a, '\n', n - a));
+    const size_t lineEnd = nl ? (size_t)(nl - base) : n;
+    size_t cut = lineEnd;
+    for (const char* q = base + a; (q = static_cast<const char*>(std::memchr(q, '/', base + lineEnd - q)));) {
+      if (q + 1 < base + lineEnd && q[1] == '/') {
+        cut = (size_t)(q - base);
+        break;
+      }
+      ++q;
+    }
     out.append(s, a, cut - a);
     out.push_back('\n');
-    if (e == std::string::npos) break;
-    a = e + 1;
+    if (!nl) break;
+    a = lineEnd + 1;
   }
   return out;
 }

@@ -94,6 +94,44 @@ def test_comments_and_headers_like_reference(tmp_path):
     assert np.array_equal(mine["cc"], ref["cc"])
 
 
+# comment layouts the reference's stripper (main.cu:533-537) handles in particular ways: a '/' and a
+# '*' left on both sides of an erased block start a new block; "//" inside a block; an unterminated
+# block keeps the rest of the file; comments between list entries
+COMMENT_EDITS = [
+    lambda s: s.replace("(\n(", "(\n//* a */* (9 9 9) */ (", 1),
+    lambda s: s.replace("(\n(", "(\n/* x // y */ // z\n(", 1),
+    lambda s: s.replace("\n(", "\n/*/ odd */(", 1),
+    lambda s: s.replace(")\n(", ")\n// between entries\n/* and */ (", 3),
+    lambda s: s.rstrip() + "\n/* never closed ( ) (\n",
+    lambda s: s.replace("FoamFile", "/*/*/ FoamFile", 1),
+]
+
+
+@needs_ref
+@pytest.mark.parametrize("edit", range(len(COMMENT_EDITS)))
+@pytest.mark.parametrize("name", ["points", "faces", "owner"])
+def test_comment_layouts_like_reference(tmp_path, edit, name):
+    m = anb.HostMesh.channel(4, 3, 2, jitter=0.1, seed=1)
+    m.write(tmp_path)
+    p = tmp_path / name
+    p.write_text(COMMENT_EDITS[edit](p.read_text()))
+    mine_err = ref_err = None
+    try:
+        mine = anb.HostMesh.read(tmp_path).geometry()
+    except Exception as e:  # noqa: BLE001
+        mine_err = str(e)
+    try:
+        ref = refshim.RefMesh(tmp_path).geometry()
+    except RuntimeError as e:
+        ref_err = str(e)
+    if ref_err is not None:
+        assert mine_err is not None and ref_err in mine_err, (mine_err, ref_err)
+        return
+    assert mine_err is None, mine_err
+    for k in ("cc", "vol", "xf", "nf", "af"):
+        assert np.array_equal(mine[k], ref[k]), k
+
+
 @needs_ref
 @pytest.mark.parametrize("name,mutate", [
     ("faces", lambda s: s.replace("4(", "4 x(", 1)),            # Malformed faces list
