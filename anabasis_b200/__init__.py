@@ -77,6 +77,7 @@ SIGNATURES = {
     "anb_create": (ct.c_int, [ct.POINTER(MeshDesc), ct.POINTER(Params), ct.POINTER(ct.c_void_p)]),
     "anb_destroy": (None, [ct.c_void_p]),
     "anb_last_error": (ct.c_char_p, [ct.c_void_p]),
+    "anb_setup_times": (ct.c_int, [ct.c_void_p, _dp]),
     "anb_get_geometry": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]),
     "anb_get_sizes": (ct.c_int, [ct.c_void_p, _ip, _ip, _ip, _ip]),
     "anb_set_bc": (ct.c_int, [ct.c_void_p, _ip, _ip, _ip, _ip, _dp, _dp, _dp, _dp]),

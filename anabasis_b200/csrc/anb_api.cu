@@ -743,11 +743,30 @@ void anb_default_params(anb_params* p) {
 
 const char* anb_last_error(const anb_ctx* c) { return c ? c->err.c_str() : g_createError.c_str(); }
 
+int anb_setup_times(const anb_ctx* c, double* t) {
+  if (!c || !t) return ANB_ERR_INVALID;
+  for (int k = 0; k < 4; ++k) t[k] = c->setupSec[k];
+  for (int k = 0; k < 6; ++k) t[4 + k] = c->L.seconds[k];
+  return ANB_OK;
+}
+
 int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
   if (!out) return ANB_ERR_INVALID;
   *out = nullptr;
   if (!md || !prm) return ANB_ERR_INVALID;
   auto c = std::make_unique<anb_ctx>();
+  auto clk = std::chrono::steady_clock::now();
+  auto lap = [&](int k) {
+    const auto t = std::chrono::steady_clock::now();
+    c->setupSec[k] = std::chrono::duration<double>(t - clk).count();
+    clk = t;
+    if (k == 2 && std::getenv("ANB_SETUP_VERBOSE")) {
+      std::fprintf(stderr, "anb_create: copy-in+topology %.3f s, geometry %.3f s, layout %.3f s [", c->setupSec[0],
+                   c->setupSec[1], c->setupSec[2]);
+      for (double s : c->L.seconds) std::fprintf(stderr, " %.3f", s);
+      std::fprintf(stderr, " ]\n");
+    }
+  };
   int rc = guarded(c.get(), [&]() -> int {
     c->prm = *prm;
     if (prm->precision != ANB_PRECISION_FP64 && prm->precision != ANB_PRECISION_MIXED)
@@ -783,7 +802,9 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     finalize_topology(m);
     for (int v : m.owner)
       if (v < 0) throw AnbError(ANB_ERR_MESH, "negative owner label");
+    lap(0);
     compute_geometry(m);
+    lap(1);
     c->L = build_layout(m);
     Layout& L = c->L;
     c->C = L.nCells;
@@ -791,6 +812,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     c->nB = L.nBoundary;
     c->nEnt = L.sliceOff.back();
     build_slot_lookup(c.get());
+    lap(2);
 
     CK(cudaSetDevice(prm->device));
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -954,6 +976,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     CK(cudaMallocHost(&c->hFlags, sizeof(int) * 32));
     CK(cudaMallocHost(&c->hScal, sizeof(double) * 64));
     CK(cudaMallocHost(&c->hStage, sizeof(double) * 3 * C));
+    CK(cudaDeviceSynchronize());
+    lap(3);
     return ANB_OK;
   });
   if (rc != ANB_OK) {

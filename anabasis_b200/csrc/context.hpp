@@ -134,6 +134,8 @@ struct anb_ctx {
   uint8_t* sBcType = nullptr;
   // steady sensitivities (adjoint_api.cu, allocated on first use)
   anb::AdjointData* adj = nullptr;
+  // anb_create wall seconds: copy-in + topology, geometry, layout, device build + upload
+  double setupSec[4] = {0, 0, 0, 0};
 };
 
 namespace anb {

@@ -176,9 +176,179 @@ inline bool parse_double(const char*& p, const char* e, double& v) {
   return true;
 }
 
+// ---- parallel parse of well-formed list bodies ---------------------------------------------
+// Large lists are cut into one chunk per thread and parsed concurrently under a strict grammar
+// (every entry complete, every token fully consumed, nothing else but whitespace).  A body that
+// passes the strict grammar everywhere is parsed by the serial readers below into exactly the
+// same values (they use the same token parsers and see the same entries in the same order), so
+// the result is identical; any deviation sends the whole file to the serial reader, whose
+// behaviour on odd input (skipped garbage, missing or extra tokens) is the reference's.
+constexpr size_t kParallelParseBytes = 1 << 20;
+
+inline bool is_ws(char c) { return std::isspace((unsigned char)c) != 0; }
+inline void skip_ws(const char*& p, const char* e) {
+  while (p < e && is_ws(*p)) ++p;
+}
+// the token just parsed ended at whitespace, ')' or the end
+inline bool token_end(const char* p, const char* e) { return p >= e || is_ws(*p) || *p == ')'; }
+
+// Chunk starts for nT threads: each cut lies just after a `sep` character (')' for lists of
+// parenthesised entries) or on whitespace (sep == 0, lists of bare labels).
+std::vector<const char*> chunk_cuts(const char* b, const char* e, int nT, char sep) {
+  std::vector<const char*> cut{b};
+  const size_t len = (size_t)(e - b);
+  for (int k = 1; k < nT; ++k) {
+    const char* q = std::max(cut.back(), b + len * (size_t)k / (size_t)nT);
+    if (sep) {
+      q = static_cast<const char*>(std::memchr(q, sep, (size_t)(e - q)));
+      q = q ? q + 1 : e;
+    } else {
+      while (q < e && !is_ws(*q)) ++q;
+    }
+    cut.push_back(q);
+  }
+  cut.push_back(e);
+  return cut;
+}
+
+int parse_threads() {
+#ifdef _OPENMP
+  return std::max(1, omp_get_max_threads());
+#else
+  return 1;
+#endif
+}
+
+// points: "(x y z)" entries
+bool parse_points_parallel(const char* b, const char* e, std::vector<Vec3>& out) {
+  const int nT = parse_threads();
+  if ((size_t)(e - b) < kParallelParseBytes || nT < 2) return false;
+  const std::vector<const char*> cut = chunk_cuts(b, e, nT, ')');
+  std::vector<std::vector<Vec3>> part(nT);
+  std::vector<char> ok(nT, 1);
+#pragma omp parallel for schedule(static, 1) num_threads(nT)
+  for (int k = 0; k < nT; ++k) {
+    const char* p = cut[k];
+    const char* ce = cut[k + 1];
+    auto& v = part[k];
+    v.reserve((size_t)(ce - p) / 40 + 1);
+    while (true) {
+      skip_ws(p, ce);
+      if (p >= ce) break;
+      if (*p != '(') { ok[k] = 0; break; }
+      ++p;
+      Vec3 x{0.0, 0.0, 0.0};
+      bool good = true;
+      for (int q = 0; q < 3 && good; ++q) good = parse_double(p, ce, x[q]) && token_end(p, ce);
+      skip_ws(p, ce);
+      if (!good || p >= ce || *p != ')') { ok[k] = 0; break; }
+      ++p;
+      v.push_back(x);
+    }
+  }
+  for (char c : ok)
+    if (!c) return false;
+  size_t n = 0;
+  for (const auto& v : part) n += v.size();
+  out.clear();
+  out.reserve(n);
+  for (const auto& v : part) out.insert(out.end(), v.begin(), v.end());
+  return true;
+}
+
+// faces: "k(v0 ... vk-1)" entries
+bool parse_faces_parallel(const char* b, const char* e, std::vector<int>& off, std::vector<int>& pts) {
+  const int nT = parse_threads();
+  if ((size_t)(e - b) < kParallelParseBytes || nT < 2) return false;
+  const std::vector<const char*> cut = chunk_cuts(b, e, nT, ')');
+  std::vector<std::vector<int>> cnt(nT), vals(nT);
+  std::vector<char> ok(nT, 1);
+#pragma omp parallel for schedule(static, 1) num_threads(nT)
+  for (int k = 0; k < nT; ++k) {
+    const char* p = cut[k];
+    const char* ce = cut[k + 1];
+    auto& c = cnt[k];
+    auto& v = vals[k];
+    c.reserve((size_t)(ce - p) / 20 + 1);
+    v.reserve((size_t)(ce - p) / 5 + 1);
+    while (true) {
+      skip_ws(p, ce);
+      if (p >= ce) break;
+      if (!std::isdigit((unsigned char)*p)) { ok[k] = 0; break; }
+      long long n = 0;
+      while (p < ce && std::isdigit((unsigned char)*p) && n < (1LL << 40)) n = n * 10 + (*p++ - '0');
+      skip_ws(p, ce);
+      if (p >= ce || *p != '(' || n >= (1LL << 31)) { ok[k] = 0; break; }
+      ++p;
+      bool good = true;
+      for (long long i = 0; i < n && good; ++i) {
+        int x = 0;
+        good = parse_int(p, ce, x) && token_end(p, ce);
+        v.push_back(x);
+      }
+      skip_ws(p, ce);
+      if (!good || p >= ce || *p != ')') { ok[k] = 0; break; }
+      ++p;
+      c.push_back((int)n);
+    }
+  }
+  for (char c : ok)
+    if (!c) return false;
+  size_t nf = 0, np = 0;
+  for (int k = 0; k < nT; ++k) {
+    nf += cnt[k].size();
+    np += vals[k].size();
+  }
+  if (np >= (size_t)INT32_MAX) return false;
+  off.assign(1, 0);
+  off.reserve(nf + 1);
+  pts.clear();
+  pts.reserve(np);
+  for (int k = 0; k < nT; ++k) {
+    for (int c : cnt[k]) off.push_back(off.back() + c);
+    pts.insert(pts.end(), vals[k].begin(), vals[k].end());
+  }
+  return true;
+}
+
+// labels: whitespace-separated integers
+bool parse_labels_parallel(const char* b, const char* e, std::vector<int>& out) {
+  const int nT = parse_threads();
+  if ((size_t)(e - b) < kParallelParseBytes || nT < 2) return false;
+  const std::vector<const char*> cut = chunk_cuts(b, e, nT, 0);
+  std::vector<std::vector<int>> part(nT);
+  std::vector<char> ok(nT, 1);
+#pragma omp parallel for schedule(static, 1) num_threads(nT)
+  for (int k = 0; k < nT; ++k) {
+    const char* p = cut[k];
+    const char* ce = cut[k + 1];
+    auto& v = part[k];
+    v.reserve((size_t)(ce - p) / 6 + 1);
+    while (true) {
+      skip_ws(p, ce);
+      if (p >= ce) break;
+      int x = 0;
+      if (!parse_int(p, ce, x) || (p < ce && !is_ws(*p))) { ok[k] = 0; break; }
+      v.push_back(x);
+    }
+  }
+  for (char c : ok)
+    if (!c) return false;
+  size_t n = 0;
+  for (const auto& v : part) n += v.size();
+  out.clear();
+  out.reserve(n);
+  for (const auto& v : part) out.insert(out.end(), v.begin(), v.end());
+  return true;
+}
+
 std::vector<Vec3> read_points(const std::string& fn) {
   std::string t = strip_comments(read_file(fn));
   auto r = main_list_range(t);
+  {
+    std::vector<Vec3> P;
+    if (parse_points_parallel(t.data() + r.first, t.data() + r.second, P)) return P;
+  }
   std::vector<Vec3> P;
   const char* base = t.data();
   size_t pos = r.first;
@@ -201,6 +371,7 @@ std::vector<Vec3> read_points(const std::string& fn) {
 void read_faces(const std::string& fn, std::vector<int>& off, std::vector<int>& pts) {
   std::string t = strip_comments(read_file(fn));
   auto r = main_list_range(t);
+  if (parse_faces_parallel(t.data() + r.first, t.data() + r.second, off, pts)) return;
   off.assign(1, 0);
   pts.clear();
   const char* base = t.data();
@@ -242,6 +413,7 @@ std::vector<int> read_labels(const std::string& fn) {
   std::string t = strip_comments(read_file(fn));
   auto r = main_list_range(t);
   std::vector<int> v;
+  if (parse_labels_parallel(t.data() + r.first, t.data() + r.second, v)) return v;
   const char* p = t.data() + r.first;
   const char* e = t.data() + r.second;
   int x;

@@ -2,6 +2,7 @@
 #include "layout.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <numeric>
 #include <queue>
@@ -83,6 +84,12 @@ Layout build_layout(const HostMesh& m) {
   L.nInternal = nI;
   L.nBoundary = nF - nI;
   L.nPatches = (int)m.patches.size();
+  auto clk = std::chrono::steady_clock::now();
+  auto lap = [&](int k) {
+    const auto t = std::chrono::steady_clock::now();
+    L.seconds[k] = std::chrono::duration<double>(t - clk).count();
+    clk = t;
+  };
 
   // unique-neighbour graph in original numbering (cellNbrs, main.cu:595-596)
   std::vector<int> off(C + 1, 0), adj;
@@ -108,6 +115,7 @@ Layout build_layout(const HostMesh& m) {
     }
   }
 
+  lap(0);
   // LSQ moment inverse per cell (build_lsq_gradient_operator, main.cu:1169-1224), original order
   std::vector<double> minvOrig((size_t)6 * C, 0.0);
   {
@@ -140,10 +148,12 @@ Layout build_layout(const HostMesh& m) {
     }
   }
 
+  lap(1);
   // RCM renumbering
   L.new2old = rcm_order(C, off, adj);
   L.old2new.assign(C, 0);
   for (int i = 0; i < C; ++i) L.old2new[L.new2old[i]] = i;
+  lap(2);
 
   // internal faces re-oriented (owner < neighbour in new ids) and sorted
   std::vector<int> fperm(nI);
@@ -196,6 +206,7 @@ Layout build_layout(const HostMesh& m) {
     L.fFlags[fi] = (uint8_t)((nd > 1e-14 ? kFaceAsm : 0) | (std::fabs(nd) > 1e-30 ? kFaceNonOrth : 0));
   }
 
+  lap(3);
   // SELL-32 pattern: row r lists its neighbours ascending with the connecting face
   std::vector<int> rOff(C + 1, 0);
   for (int fi = 0; fi < nI; ++fi) {
@@ -249,6 +260,7 @@ Layout build_layout(const HostMesh& m) {
     }
   }
 
+  lap(4);
   // boundary faces (input order)
   const int nB = nF - nI;
   L.bOwner.resize(nB);
@@ -292,6 +304,7 @@ Layout build_layout(const HostMesh& m) {
     for (int k = 0; k < 3; ++k) L.cc[(size_t)3 * r + k] = m.cc[o][k];
     for (int k = 0; k < 6; ++k) L.minv[(size_t)6 * r + k] = minvOrig[(size_t)6 * o + k];
   }
+  lap(5);
   return L;
 }
 

@@ -30,6 +30,9 @@ enum FaceFlag : uint8_t {
 
 struct Layout {
   int nCells = 0, nInternal = 0, nBoundary = 0, nPatches = 0;
+  // wall seconds of the build: adjacency, LSQ moments, RCM, face order + coefficients, SELL pattern,
+  // boundary faces + cell data
+  double seconds[6] = {0, 0, 0, 0, 0, 0};
   std::vector<int> new2old, old2new;  // cells
 
   // SELL-32 off-diagonal pattern

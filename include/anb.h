@@ -103,6 +103,11 @@ void anb_default_params(anb_params* p);
 int anb_create(const anb_mesh_desc* mesh, const anb_params* params, anb_ctx** out);
 void anb_destroy(anb_ctx* ctx);
 const char* anb_last_error(const anb_ctx* ctx);
+/* Wall seconds of anb_create (no counterpart in the reference): t[0] copy-in and topology, t[1]
+ * geometry, t[2] device layout (RCM, SELL-32, face coefficients, LSQ moments), t[3] device
+ * allocation and upload; t[4..9] the layout's parts (adjacency, LSQ moments, RCM, face order and
+ * coefficients, SELL-32 pattern, boundary faces and cell data). */
+int anb_setup_times(const anb_ctx* ctx, double t[10]);
 
 /* Cell/face geometry in input numbering (any pointer may be NULL).  cc, xf, nf: 3 per entry. */
 int anb_get_geometry(anb_ctx* ctx, double* cc, double* vol, double* xf, double* nf, double* area,

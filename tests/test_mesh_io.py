@@ -132,6 +132,56 @@ def test_comment_layouts_like_reference(tmp_path, edit, name):
         assert np.array_equal(mine[k], ref[k]), k
 
 
+def _mid_replace(s, old, new):
+    """Replaces the first `old` after the middle of `s` (inside a large list)."""
+    i = s.index(old, len(s) // 2)
+    return s[:i] + new + s[i + len(old):]
+
+
+# large files (several MB) are parsed in parallel chunks under a strict grammar; entries that
+# leave it (extra tokens, trailing garbage, signs, comments) send the file to the serial reader
+LARGE_EDITS = [
+    ("points", None),
+    ("points", lambda s: _mid_replace(s, ")\n(", " 7)\n(")),            # a fourth coordinate
+    ("points", lambda s: _mid_replace(s, ")\n(", ")\n junk (")),        # garbage between entries
+    ("faces", lambda s: _mid_replace(s, ")\n4(", " 5)\n4(")),          # an extra vertex
+    ("faces", lambda s: _mid_replace(s, "\n4(", "\n// note\n4(")),      # a comment inside the list
+    ("owner", lambda s: _mid_replace(s, "\n", "\n+3 ")),                 # a signed label
+    ("neighbour", lambda s: _mid_replace(s, "\n", "\nx ")),              # a label list cut short
+]
+
+
+@needs_ref
+@pytest.mark.parametrize("name,mutate", LARGE_EDITS)
+def test_large_files_like_reference(tmp_path, name, mutate):
+    m = anb.HostMesh.channel(60, 40, 40, jitter=0.1, seed=3)
+    m.write(tmp_path)
+    p = tmp_path / name
+    assert p.stat().st_size > 2 << 20 or name in ("owner", "neighbour")
+    if mutate is not None:
+        p.write_text(mutate(p.read_text()))
+    mine_err = ref_err = None
+    try:
+        r = anb.HostMesh.read(tmp_path)
+        mine = r.geometry()
+    except Exception as e:  # noqa: BLE001
+        mine_err = str(e)
+    try:
+        ref = refshim.RefMesh(tmp_path).geometry()
+    except RuntimeError as e:
+        ref_err = str(e)
+    if ref_err is not None:
+        assert mine_err is not None and ref_err in mine_err, (mine_err, ref_err)
+        return
+    assert mine_err is None, mine_err
+    for k in ("cc", "vol", "xf", "nf", "af"):
+        assert np.array_equal(mine[k], ref[k]), k
+    if mutate is None:
+        a, b = m.topology(), r.topology()
+        for k in ("points", "face_offsets", "face_points", "owner", "neighbour"):
+            assert np.array_equal(a[k], b[k]), k
+
+
 @needs_ref
 @pytest.mark.parametrize("name,mutate", [
     ("faces", lambda s: s.replace("4(", "4 x(", 1)),            # Malformed faces list
