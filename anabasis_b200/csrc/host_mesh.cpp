@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <cctype>
+#include <climits>
 #include <cerrno>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -49,12 +51,14 @@ std::string read_file(const std::string& fn) {
 // linear pass each.  The reference erases the first "/*" ... "*/" block and searches the edited
 // string again from its start, so a '/' just before an erased block and a '*' just after it form a
 // new block start; the scan below reproduces that.
-std::string strip_comments(const std::string& txt) {
+std::string strip_comments(std::string txt) {
   const size_t npos = std::string::npos;
   std::string s;
-  s.reserve(txt.size());
   size_t i = 0;
-  while (true) {
+  const bool blocks = txt.find("/*") != npos;
+  if (!blocks) s = std::move(txt);  // no block comment: nothing to erase
+  else s.reserve(txt.size());
+  while (blocks) {
     const size_t a = txt.find("/*", i);
     if (a == npos) {
       s.append(txt, i, npos);
@@ -81,28 +85,37 @@ std::string strip_comments(const std::string& txt) {
     }
     if (stop) break;
   }
+  // line comments: each line keeps what precedes its first "//" and ends with '\n' (the
+  // reference's getline loop); lines without "//" are copied in bulk up to the next occurrence
   std::string out;
   out.reserve(s.size() + 1);
-  const char* base = s.data();
   const size_t n = s.size();
   size_t a = 0;
   while (a < n) {
-    const char* nl = static_cast<const char*>(std::memchr(base + a, '\n', n - a));
-    const size_t lineEnd = nl ? (size_t)(nl - base) : n;
-    size_t cut = lineEnd;
-    for (const char* q = base + a; (q = static_cast<const char*>(std::memchr(q, '/', base + lineEnd - q)));) {
-      if (q + 1 < base + lineEnd && q[1] == '/') {
-        cut = (size_t)(q - base);
-        break;
-      }
-      ++q;
+    const size_t c = s.find("//", a);
+    if (c == npos) {
+      out.append(s, a, npos);
+      if (out.back() != '\n') out.push_back('\n');
+      break;
     }
-    out.append(s, a, cut - a);
+    out.append(s, a, c - a);
     out.push_back('\n');
-    if (!nl) break;
-    a = lineEnd + 1;
+    const size_t nl = s.find('\n', c);
+    if (nl == npos) break;
+    a = nl + 1;
   }
   return out;
+}
+
+// files (list bodies) larger than this are scanned and parsed by all host threads
+constexpr size_t kParallelParseBytes = 1 << 20;
+
+int parse_threads() {
+#ifdef _OPENMP
+  return std::max(1, omp_get_max_threads());
+#else
+  return 1;
+#endif
 }
 
 // First "<digits> (" opens the top-level list; returns its inside (main.cu:538-546).
@@ -121,9 +134,43 @@ std::pair<size_t, size_t> main_list_range(const std::string& t) {
     }
   }
   if (start == std::string::npos) throw std::runtime_error("Could not locate top-level OpenFOAM list");
-  int depth = 0;
+  // the matching ')' is the first position where the running depth (1 after the opening '(')
+  // returns to 0; large files are scanned in chunks: the net depth change and the lowest running
+  // depth of each chunk in parallel, then the first chunk whose lowest depth reaches 0 is scanned
+  // again from its starting depth for the exact position
+  const size_t n = t.size();
   size_t close = std::string::npos;
-  for (size_t i = open; i < t.size(); ++i) {
+  const int nT = parse_threads();
+  size_t from = open;
+  long long depth = 0;
+  if (n - open > kParallelParseBytes && nT > 1) {
+    const int nC = 4 * nT;
+    const size_t len = n - open;
+    std::vector<long long> net(nC, 0), low(nC, 0);
+#pragma omp parallel for schedule(static) num_threads(nT)
+    for (int k = 0; k < nC; ++k) {
+      const size_t b = open + len * (size_t)k / nC, e = open + len * (size_t)(k + 1) / nC;
+      long long d = 0, lo = LLONG_MAX;
+      for (size_t i = b; i < e; ++i) {
+        const char c = t[i];
+        d += (c == '(') - (c == ')');
+        lo = std::min(lo, d);
+      }
+      net[k] = d;
+      low[k] = lo;
+    }
+    from = n;  // no chunk closes: nothing to scan, "Failed to match parentheses" below
+    long long base = 0;
+    for (int k = 0; k < nC; ++k) {
+      if (low[k] != LLONG_MAX && base + low[k] <= 0) {
+        from = open + len * (size_t)k / nC;
+        depth = base;
+        break;
+      }
+      base += net[k];
+    }
+  }
+  for (size_t i = from; i < n; ++i) {
     if (t[i] == '(') ++depth;
     else if (t[i] == ')') {
       --depth;
@@ -183,12 +230,29 @@ inline bool parse_double(const char*& p, const char* e, double& v) {
 // same values (they use the same token parsers and see the same entries in the same order), so
 // the result is identical; any deviation sends the whole file to the serial reader, whose
 // behaviour on odd input (skipped garbage, missing or extra tokens) is the reference's.
-constexpr size_t kParallelParseBytes = 1 << 20;
 
-inline bool is_ws(char c) { return std::isspace((unsigned char)c) != 0; }
+// the C locale's isspace set: ' ', \t, \n, \v, \f, \r
+inline bool is_ws(char c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
 inline void skip_ws(const char*& p, const char* e) {
   while (p < e && is_ws(*p)) ++p;
 }
+// parse_int for the strict paths (same result; the C locale's whitespace set inline)
+inline bool parse_int_fast(const char*& p, const char* e, int& v) {
+  while (p < e && is_ws(*p)) ++p;
+  const char* q = p;
+  bool neg = false;
+  if (q < e && (*q == '-' || *q == '+')) {
+    neg = (*q == '-');
+    ++q;
+  }
+  if (q >= e || (unsigned)(*q - '0') > 9u) return false;
+  long long acc = 0;
+  while (q < e && (unsigned)(*q - '0') <= 9u) acc = acc * 10 + (*q++ - '0');
+  v = (int)(neg ? -acc : acc);
+  p = q;
+  return true;
+}
+
 // the token just parsed ended at whitespace, ')' or the end
 inline bool token_end(const char* p, const char* e) { return p >= e || is_ws(*p) || *p == ')'; }
 
@@ -211,12 +275,15 @@ std::vector<const char*> chunk_cuts(const char* b, const char* e, int nT, char s
   return cut;
 }
 
-int parse_threads() {
-#ifdef _OPENMP
-  return std::max(1, omp_get_max_threads());
-#else
-  return 1;
-#endif
+// out = the chunks' vectors one after the other, copied in parallel
+template <class T>
+void concat_parallel(const std::vector<std::vector<T>>& part, std::vector<T>& out) {
+  std::vector<size_t> at(part.size() + 1, 0);
+  for (size_t k = 0; k < part.size(); ++k) at[k + 1] = at[k] + part[k].size();
+  out.resize(at.back());
+#pragma omp parallel for schedule(static, 1)
+  for (int k = 0; k < (int)part.size(); ++k)
+    if (!part[k].empty()) std::memcpy(out.data() + at[k], part[k].data(), part[k].size() * sizeof(T));
 }
 
 // points: "(x y z)" entries
@@ -248,11 +315,7 @@ bool parse_points_parallel(const char* b, const char* e, std::vector<Vec3>& out)
   }
   for (char c : ok)
     if (!c) return false;
-  size_t n = 0;
-  for (const auto& v : part) n += v.size();
-  out.clear();
-  out.reserve(n);
-  for (const auto& v : part) out.insert(out.end(), v.begin(), v.end());
+  concat_parallel(part, out);
   return true;
 }
 
@@ -283,7 +346,7 @@ bool parse_faces_parallel(const char* b, const char* e, std::vector<int>& off, s
       bool good = true;
       for (long long i = 0; i < n && good; ++i) {
         int x = 0;
-        good = parse_int(p, ce, x) && token_end(p, ce);
+        good = parse_int_fast(p, ce, x) && token_end(p, ce);
         v.push_back(x);
       }
       skip_ws(p, ce);
@@ -300,14 +363,12 @@ bool parse_faces_parallel(const char* b, const char* e, std::vector<int>& off, s
     np += vals[k].size();
   }
   if (np >= (size_t)INT32_MAX) return false;
-  off.assign(1, 0);
-  off.reserve(nf + 1);
-  pts.clear();
-  pts.reserve(np);
-  for (int k = 0; k < nT; ++k) {
-    for (int c : cnt[k]) off.push_back(off.back() + c);
-    pts.insert(pts.end(), vals[k].begin(), vals[k].end());
-  }
+  concat_parallel(vals, pts);
+  std::vector<int> sizes;
+  concat_parallel(cnt, sizes);
+  off.resize(nf + 1);
+  off[0] = 0;
+  for (size_t f = 0; f < nf; ++f) off[f + 1] = off[f] + sizes[f];
   return true;
 }
 
@@ -328,17 +389,13 @@ bool parse_labels_parallel(const char* b, const char* e, std::vector<int>& out) 
       skip_ws(p, ce);
       if (p >= ce) break;
       int x = 0;
-      if (!parse_int(p, ce, x) || (p < ce && !is_ws(*p))) { ok[k] = 0; break; }
+      if (!parse_int_fast(p, ce, x) || (p < ce && !is_ws(*p))) { ok[k] = 0; break; }
       v.push_back(x);
     }
   }
   for (char c : ok)
     if (!c) return false;
-  size_t n = 0;
-  for (const auto& v : part) n += v.size();
-  out.clear();
-  out.reserve(n);
-  for (const auto& v : part) out.insert(out.end(), v.begin(), v.end());
+  concat_parallel(part, out);
   return true;
 }
 
@@ -643,13 +700,28 @@ void compute_geometry(HostMesh& m, int nThreads) {
 
 HostMesh read_polymesh(const std::string& dir) {
   HostMesh m;
+  auto clk = std::chrono::steady_clock::now();
+  double sec[5];
+  auto lap = [&](int k) {
+    const auto t = std::chrono::steady_clock::now();
+    sec[k] = std::chrono::duration<double>(t - clk).count();
+    clk = t;
+  };
   m.patches = read_boundary(dir + "/boundary");
   m.points = read_points(dir + "/points");
+  lap(0);
   read_faces(dir + "/faces", m.faceOff, m.facePts);
+  lap(1);
   m.owner = read_labels(dir + "/owner");
   m.neigh = read_labels(dir + "/neighbour");
+  lap(2);
   finalize_topology(m);
+  lap(3);
   compute_geometry(m);
+  lap(4);
+  if (std::getenv("ANB_SETUP_VERBOSE"))
+    std::fprintf(stderr, "read_polymesh: points %.3f s, faces %.3f s, labels %.3f s, topology %.3f s, geometry %.3f s\n",
+                 sec[0], sec[1], sec[2], sec[3], sec[4]);
   return m;
 }
 
