@@ -28,7 +28,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SOURCES = ["host_mesh.cpp", "host_case.cpp", "host_output.cpp", "host_api.cpp", "layout.cpp", "amg_setup.cpp"]
 MMS_APPS = {1: "anabasis_poisson_mms", 2: "anabasis_poisson_mms_neumann", 3: "anabasis_poisson_mms_mixed",
             4: "anabasis_scalar_mms"}
-CUDA_SOURCES = ["kernels_fv.cu", "kernels_krylov.cu", "kernels_scalar.cu", "kernels_adjoint.cu", "anb_api.cu", "adjoint_api.cu", "nalloc.cu"]
+CUDA_SOURCES = ["kernels_fv.cu", "kernels_krylov.cu", "kernels_scalar.cu", "kernels_adjoint.cu", "anb_api.cu", "adjoint_api.cu", "nalloc.cu",
+                "setup_gpu.cu"]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
 NVCCFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp", "--expt-relaxed-constexpr"]
 

@@ -11,6 +11,7 @@
 
 #include "context.hpp"
 #include "context_access.hpp"
+#include "setup_gpu.hpp"
 
 namespace anb {
 
@@ -297,12 +298,6 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
     d.x2 = ar.alloc<T>(h.n);
     if (l + 1 < A.nLevels) {
       d.agg = ar.upload(h.agg);
-      if (l == 0 || !h.sliceOff.empty()) {  // SELL level: the aggregate of every slot's column
-        const std::vector<int>& col = l == 0 ? c->L.col : h.col;
-        std::vector<int> sa(col.size());
-        for (size_t e = 0; e < col.size(); ++e) sa[e] = h.agg[col[e]];
-        d.slotAgg = ar.upload(sa);
-      }
       d.memOff = ar.upload(h.memOff);
       d.mem = ar.upload(h.mem);
       d.gOff = ar.upload(h.gOff);
@@ -803,9 +798,27 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     for (int v : m.owner)
       if (v < 0) throw AnbError(ANB_ERR_MESH, "negative owner label");
     lap(0);
-    compute_geometry(m);
+    CK(cudaSetDevice(prm->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    if (nalloc_prepare_device(prm->device) != 0)
+      throw AnbError(ANB_ERR_CUDA, "could not place the static scratch of anb_patch_force_nalloc on the device");
+    // geometry, LSQ moments and slot-ordered face records on the device (bit-identical to the
+    // host restatement; ANB_HOST_SETUP=1 builds them on the host instead)
+    const char* hs = std::getenv("ANB_HOST_SETUP");
+    const bool hostSetup = hs && hs[0] == '1';
+    if (hostSetup || !compute_geometry_gpu(m, c->stream)) compute_geometry(m);
     lap(1);
-    c->L = build_layout(m);
+    {
+      auto t0 = std::chrono::steady_clock::now();
+      std::vector<int> adjOff, adj;
+      cell_adjacency(m, adjOff, adj);
+      auto t1 = std::chrono::steady_clock::now();
+      const std::vector<double> minv = hostSetup ? lsq_minv_host(m, adjOff, adj) : lsq_minv_gpu(m, adjOff, adj, c->stream);
+      auto t2 = std::chrono::steady_clock::now();
+      c->L = build_layout(m, adjOff, adj, minv);
+      c->L.seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+      c->L.seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    }
     Layout& L = c->L;
     c->C = L.nCells;
     c->nI = L.nInternal;
@@ -814,10 +827,6 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     build_slot_lookup(c.get());
     lap(2);
 
-    CK(cudaSetDevice(prm->device));
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    if (nalloc_prepare_device(prm->device) != 0)
-      throw AnbError(ANB_ERR_CUDA, "could not place the static scratch of anb_patch_force_nalloc on the device");
     int nSM = 148;
     CK(cudaDeviceGetAttribute(&nSM, cudaDevAttrMultiProcessorCount, prm->device));
     c->lc.stream = c->stream;
@@ -876,19 +885,27 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     dm.fFlags = A.upload(L.fFlags);
     {
       const size_t nE = (size_t)c->nEnt;
-      std::vector<double> sg(8 * nE, 0.0);
-      std::vector<uint8_t> sf(nE, 0);
-      for (size_t e = 0; e < nE; ++e) {
-        const int f = L.slotFace[e];
-        if (f < 0) continue;
-        const FaceRec& r = fr[f];
-        const double v[8] = {r.lam, r.g, r.t[0], r.t[1], r.t[2], r.d[0], r.d[1], r.d[2]};
-        for (int q = 0; q < 8; ++q) sg[q * nE + e] = v[q];
-        sf[e] = L.fFlags[f];
-      }
       dm.nEnt = c->nEnt;
-      dm.slotGeom = A.upload(sg);
-      dm.slotFlags = A.upload(sf);
+      if (hostSetup) {
+        std::vector<double> sg(8 * nE, 0.0);
+        std::vector<uint8_t> sf(nE, 0);
+        for (size_t e = 0; e < nE; ++e) {
+          const int f = L.slotFace[e];
+          if (f < 0) continue;
+          const FaceRec& r = fr[f];
+          const double v[8] = {r.lam, r.g, r.t[0], r.t[1], r.t[2], r.d[0], r.d[1], r.d[2]};
+          for (int q = 0; q < 8; ++q) sg[q * nE + e] = v[q];
+          sf[e] = L.fFlags[f];
+        }
+        dm.slotGeom = A.upload(sg);
+        dm.slotFlags = A.upload(sf);
+      } else {
+        double* sg = A.alloc<double>(8 * nE);
+        uint8_t* sf = A.alloc<uint8_t>(nE);
+        build_slot_geometry(nE, dm.slotFace, c->dFace, dm.fFlags, sg, sf, c->stream);
+        dm.slotGeom = sg;
+        dm.slotFlags = sf;
+      }
     }
     dm.bOwner = A.upload(L.bOwner);
     dm.bnd = c->dBnd;

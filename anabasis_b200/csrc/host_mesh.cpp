@@ -687,6 +687,10 @@ void compute_geometry(HostMesh& m, int nThreads) {
     m.Sf[f] = mul3(areaMag, nloc);
   }
   if (badFace >= 0) throw std::runtime_error("Degenerate face area at face " + std::to_string(badFace));
+  max_nonorth_deg(m);
+}
+
+void max_nonorth_deg(HostMesh& m) {
   double mx = 0.0;
 #pragma omp parallel for reduction(max : mx) schedule(static)
   for (int f = 0; f < m.nInternalFaces; ++f) {

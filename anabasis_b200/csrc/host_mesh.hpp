@@ -57,6 +57,8 @@ void write_polymesh(const HostMesh& m, const std::string& polyMeshDir);
 // "Non-positive cell volume at cell N" / "Degenerate face area at face N".
 void finalize_topology(HostMesh& m);
 void compute_geometry(HostMesh& m, int nThreads = 0);
+// Largest angle between an internal face normal and its cell-centre vector, in degrees (main.cu:598).
+void max_nonorth_deg(HostMesh& m);
 
 struct ChannelSpec {
   int nx = 40, ny = 20, nz = 20;

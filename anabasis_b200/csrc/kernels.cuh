@@ -262,7 +262,6 @@ struct AmgLevelDevT {
   const int* mem;
   const int* gOff;     // Galerkin gather for the next level's storage
   const int* gIdx;
-  const int* slotAgg;  // SELL levels: aggregate of each storage slot's column, agg[col[e]]
   int nEntNext;        // next level's SELL storage entries
   // work vectors
   T *b, *x, *x2;

@@ -739,29 +739,15 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
       for (int k = 0; k < W; ++k) {
         const int ee = b + (k << 5);
         const int j = __ldg(&f.col[ee]);
-        ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.slotAgg[ee])]));
+        ax += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
       }
     } else {
-      // column, value and the column's aggregate of every slot first (no col -> agg load chain);
-      // slots past the row's width read as (row i, value 0, aggregate of row i)
-      const int s = i >> 5;
-      const int b0 = __ldg(&f.sliceOff[s]);
-      const int W = (__ldg(&f.sliceOff[s + 1]) - b0) >> 5;
-      const int base = b0 + (i & 31);
-      const int gi = __ldg(&f.agg[i]);
-      int c[WM], g[WM];
+      int c[WM];
       double v[WM];
+      sell_regs<WM>(f.sliceOff, f.col, f.val, i, c, v);
+      int g[WM];
 #pragma unroll
-      for (int k = 0; k < WM; ++k) {
-        c[k] = i;
-        g[k] = gi;
-        v[k] = 0.0;
-        if (k < W) {
-          c[k] = __ldg(&f.col[base + (k << 5)]);
-          g[k] = __ldg(&f.slotAgg[base + (k << 5)]);
-          v[k] = ld(&f.val[base + (k << 5)]);
-        }
-      }
+      for (int k = 0; k < WM; ++k) g[k] = __ldg(&f.agg[c[k]]);
 #pragma unroll
       for (int k = 0; k < WM; ++k) ax += v[k] * (ld(&f.x[c[k]]) + corr * ld(&e[g[k]]));
     }

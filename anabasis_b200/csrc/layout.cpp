@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <numeric>
 #include <queue>
@@ -77,7 +78,75 @@ std::vector<int> rcm_order(int n, const std::vector<int>& off, const std::vector
   return order;
 }
 
+void cell_adjacency(const HostMesh& m, std::vector<int>& off, std::vector<int>& adj) {
+  const int C = m.nCells, nI = m.nInternalFaces;
+  off.assign(C + 1, 0);
+  std::vector<int> cnt(C + 1, 0);
+  for (int f = 0; f < nI; ++f) {
+    cnt[m.owner[f] + 1]++;
+    cnt[m.neigh[f] + 1]++;
+  }
+  for (int c = 0; c < C; ++c) off[c + 1] = off[c] + cnt[c + 1];
+  adj.assign(off[C], 0);
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (int f = 0; f < nI; ++f) {
+    adj[fill[m.owner[f]]++] = m.neigh[f];
+    adj[fill[m.neigh[f]]++] = m.owner[f];
+  }
+  int dup = -1;
+#pragma omp parallel for schedule(static) reduction(max : dup)
+  for (int c = 0; c < C; ++c) {
+    auto b = adj.begin() + off[c], e = adj.begin() + off[c + 1];
+    std::sort(b, e);
+    if (std::adjacent_find(b, e) != e) dup = std::max(dup, C - 1 - c);  // keep the lowest such cell
+  }
+  if (dup >= 0)
+    throw std::runtime_error("cell " + std::to_string(C - 1 - dup) +
+                             " shares more than one internal face with a neighbour (unsupported)");
+}
+
+std::vector<double> lsq_minv_host(const HostMesh& m, const std::vector<int>& off, const std::vector<int>& adj) {
+  const int C = m.nCells, nI = m.nInternalFaces, nF = m.nFaces;
+  std::vector<double> minvOrig((size_t)6 * C, 0.0);
+  std::vector<std::vector<int>> cellB(C);
+  for (int f = nI; f < nF; ++f) cellB[m.owner[f]].push_back(f);
+#pragma omp parallel for schedule(static)
+  for (int P = 0; P < C; ++P) {
+    const Vec3 xP = m.cc[P];
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    auto acc = [&](const Vec3& x) {
+      double r[3] = {x[0] - xP[0], x[1] - xP[1], x[2] - xP[2]};
+      double w = 1.0 / std::max(r[0] * r[0] + r[1] * r[1] + r[2] * r[2], 1e-30);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) M[i][j] += w * r[i] * r[j];
+    };
+    for (int k = off[P]; k < off[P + 1]; ++k) acc(m.cc[adj[k]]);
+    for (int f : cellB[P]) acc(m.xf[f]);
+    double a = M[0][0], b = M[0][1], c = M[0][2], d = M[1][0], e = M[1][1], f2 = M[1][2], g = M[2][0],
+           h = M[2][1], k = M[2][2];
+    double det = a * (e * k - f2 * h) - b * (d * k - f2 * g) + c * (d * h - e * g);
+    double* o = &minvOrig[(size_t)6 * P];
+    if (std::fabs(det) > 1e-20) {
+      o[0] = (e * k - f2 * h) / det;
+      o[1] = (c * h - b * k) / det;
+      o[2] = (b * f2 - c * e) / det;
+      o[3] = (a * k - c * g) / det;
+      o[4] = (c * d - a * f2) / det;
+      o[5] = (a * e - b * d) / det;
+    }
+  }
+  return minvOrig;
+}
+
 Layout build_layout(const HostMesh& m) {
+  std::vector<int> off, adj;
+  cell_adjacency(m, off, adj);
+  const std::vector<double> minv = lsq_minv_host(m, off, adj);
+  return build_layout(m, off, adj, minv);
+}
+
+Layout build_layout(const HostMesh& m, const std::vector<int>& off, const std::vector<int>& adj,
+                    const std::vector<double>& minvOrig) {
   Layout L;
   const int C = m.nCells, nI = m.nInternalFaces, nF = m.nFaces;
   L.nCells = C;
@@ -90,64 +159,7 @@ Layout build_layout(const HostMesh& m) {
     L.seconds[k] = std::chrono::duration<double>(t - clk).count();
     clk = t;
   };
-
-  // unique-neighbour graph in original numbering (cellNbrs, main.cu:595-596)
-  std::vector<int> off(C + 1, 0), adj;
-  {
-    std::vector<int> cnt(C + 1, 0);
-    for (int f = 0; f < nI; ++f) {
-      cnt[m.owner[f] + 1]++;
-      cnt[m.neigh[f] + 1]++;
-    }
-    for (int c = 0; c < C; ++c) off[c + 1] = off[c] + cnt[c + 1];
-    adj.assign(off[C], 0);
-    std::vector<int> fill(off.begin(), off.end() - 1);
-    for (int f = 0; f < nI; ++f) {
-      adj[fill[m.owner[f]]++] = m.neigh[f];
-      adj[fill[m.neigh[f]]++] = m.owner[f];
-    }
-    for (int c = 0; c < C; ++c) {
-      auto b = adj.begin() + off[c], e = adj.begin() + off[c + 1];
-      std::sort(b, e);
-      if (std::adjacent_find(b, e) != e)
-        throw std::runtime_error("cell " + std::to_string(c) +
-                                 " shares more than one internal face with a neighbour (unsupported)");
-    }
-  }
-
   lap(0);
-  // LSQ moment inverse per cell (build_lsq_gradient_operator, main.cu:1169-1224), original order
-  std::vector<double> minvOrig((size_t)6 * C, 0.0);
-  {
-    std::vector<std::vector<int>> cellB(C);
-    for (int f = nI; f < nF; ++f) cellB[m.owner[f]].push_back(f);
-#pragma omp parallel for schedule(static)
-    for (int P = 0; P < C; ++P) {
-      const Vec3 xP = m.cc[P];
-      double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      auto acc = [&](const Vec3& x) {
-        double r[3] = {x[0] - xP[0], x[1] - xP[1], x[2] - xP[2]};
-        double w = 1.0 / std::max(r[0] * r[0] + r[1] * r[1] + r[2] * r[2], 1e-30);
-        for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j) M[i][j] += w * r[i] * r[j];
-      };
-      for (int k = off[P]; k < off[P + 1]; ++k) acc(m.cc[adj[k]]);
-      for (int f : cellB[P]) acc(m.xf[f]);
-      double a = M[0][0], b = M[0][1], c = M[0][2], d = M[1][0], e = M[1][1], f2 = M[1][2], g = M[2][0],
-             h = M[2][1], k = M[2][2];
-      double det = a * (e * k - f2 * h) - b * (d * k - f2 * g) + c * (d * h - e * g);
-      double* o = &minvOrig[(size_t)6 * P];
-      if (std::fabs(det) > 1e-20) {
-        o[0] = (e * k - f2 * h) / det;
-        o[1] = (c * h - b * k) / det;
-        o[2] = (b * f2 - c * e) / det;
-        o[3] = (a * k - c * g) / det;
-        o[4] = (c * d - a * f2) / det;
-        o[5] = (a * e - b * d) / det;
-      }
-    }
-  }
-
   lap(1);
   // RCM renumbering
   L.new2old = rcm_order(C, off, adj);
@@ -155,16 +167,25 @@ Layout build_layout(const HostMesh& m) {
   for (int i = 0; i < C; ++i) L.old2new[L.new2old[i]] = i;
   lap(2);
 
-  // internal faces re-oriented (owner < neighbour in new ids) and sorted
+  // internal faces re-oriented (owner < neighbour in new ids) and ordered by (owner, neighbour):
+  // counted into owner buckets, each bucket sorted by neighbour (pairs are distinct)
   std::vector<int> fperm(nI);
-  std::iota(fperm.begin(), fperm.end(), 0);
-  std::vector<long long> key(nI);
-  for (int f = 0; f < nI; ++f) {
-    int a = L.old2new[m.owner[f]], b = L.old2new[m.neigh[f]];
-    if (a > b) std::swap(a, b);
-    key[f] = (long long)a * C + b;
+  {
+    std::vector<int> lo(nI), hi(nI), bOff(C + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (int f = 0; f < nI; ++f) {
+      const int a = L.old2new[m.owner[f]], b = L.old2new[m.neigh[f]];
+      lo[f] = std::min(a, b);
+      hi[f] = std::max(a, b);
+    }
+    for (int f = 0; f < nI; ++f) bOff[lo[f] + 1]++;
+    for (int r = 0; r < C; ++r) bOff[r + 1] += bOff[r];
+    std::vector<int> fill(bOff.begin(), bOff.end() - 1);
+    for (int f = 0; f < nI; ++f) fperm[fill[lo[f]]++] = f;
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < C; ++r)
+      std::sort(fperm.begin() + bOff[r], fperm.begin() + bOff[r + 1], [&](int x, int y) { return hi[x] < hi[y]; });
   }
-  std::sort(fperm.begin(), fperm.end(), [&](int x, int y) { return key[x] < key[y]; });
   L.fOwner.resize(nI);
   L.fNeigh.resize(nI);
   L.fOrig.resize(nI);
@@ -243,6 +264,7 @@ Layout build_layout(const HostMesh& m) {
   }
   L.col.assign(L.sliceOff[L.nSlices], 0);
   L.slotFace.assign(L.sliceOff[L.nSlices], -1);
+#pragma omp parallel for schedule(static)
   for (int s = 0; s < L.nSlices; ++s) {
     const int w = (L.sliceOff[s + 1] - L.sliceOff[s]) / kSlice;
     for (int lane = 0; lane < kSlice; ++lane) {
@@ -269,12 +291,14 @@ Layout build_layout(const HostMesh& m) {
   L.bT.resize((size_t)3 * nB);
   L.bS.resize((size_t)3 * nB);
   L.bFlags.resize(nB);
+  int noPatch = INT_MAX;
+#pragma omp parallel for schedule(static) reduction(min : noPatch)
   for (int b = 0; b < nB; ++b) {
     const int f = nI + b;
     const int P = m.owner[f];
     L.bOwner[b] = L.old2new[P];
     L.bPatch[b] = m.bPatch[f] - 1;
-    if (L.bPatch[b] < 0) throw std::runtime_error("boundary face " + std::to_string(f) + " belongs to no patch");
+    if (L.bPatch[b] < 0) noPatch = std::min(noPatch, f);
     const double d[3] = {m.xf[f][0] - m.cc[P][0], m.xf[f][1] - m.cc[P][1], m.xf[f][2] - m.cc[P][2]};
     const double nd = m.nf[f][0] * d[0] + m.nf[f][1] * d[1] + m.nf[f][2] * d[2];
     const double g = m.Af[f] / std::max(std::fabs(nd), 1e-30);
@@ -285,6 +309,7 @@ Layout build_layout(const HostMesh& m) {
     }
     L.bFlags[b] = (uint8_t)((nd > 1e-14 ? kFaceAsm : 0) | (std::fabs(nd) > 1e-30 ? kFaceNonOrth : 0));
   }
+  if (noPatch != INT_MAX) throw std::runtime_error("boundary face " + std::to_string(noPatch) + " belongs to no patch");
   L.cbOff.assign(C + 1, 0);
   for (int b = 0; b < nB; ++b) L.cbOff[L.bOwner[b] + 1]++;
   for (int r = 0; r < C; ++r) L.cbOff[r + 1] += L.cbOff[r];
@@ -298,6 +323,7 @@ Layout build_layout(const HostMesh& m) {
   L.vol.resize(C);
   L.cc.resize((size_t)3 * C);
   L.minv.resize((size_t)6 * C);
+#pragma omp parallel for schedule(static)
   for (int r = 0; r < C; ++r) {
     const int o = L.new2old[r];
     L.vol[r] = m.vol[o];

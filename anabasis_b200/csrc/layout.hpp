@@ -65,6 +65,16 @@ struct Layout {
 };
 
 // Throws std::runtime_error when two internal faces join the same pair of cells (not supported).
+// Distinct neighbours of every cell, ascending, in input numbering (cellNbrs, main.cu:595-596);
+// throws when two internal faces join the same pair of cells.
+void cell_adjacency(const HostMesh& m, std::vector<int>& off, std::vector<int>& adj);
+// LSQ moment inverse (build_lsq_gradient_operator, main.cu:1169-1224), 6 per cell in input
+// numbering, on the host.
+std::vector<double> lsq_minv_host(const HostMesh& m, const std::vector<int>& off, const std::vector<int>& adj);
+// The device layout from the mesh, its adjacency and its moment inverses (input numbering).
+Layout build_layout(const HostMesh& m, const std::vector<int>& off, const std::vector<int>& adj,
+                    const std::vector<double>& minvOrig);
+// Same, with the adjacency and moments computed on the host.
 Layout build_layout(const HostMesh& m);
 
 // LSQ moment inverse of the scalar libraries (libpoisson/src/gradient.cu:21-83,

@@ -80,8 +80,8 @@ def _library_vs_oracle(m, bc, steps, tight, force_patch):
     got = np.array(f["Fp"] + f["Fv"] + f["F"])
     assert np.abs(got - fo[:9]).max() <= 1e-8 * np.abs(fo[:9]).max()
     # the monitors of every step
-    for a, b in zip(st, rst):
-        assert abs(a["du_rel"] - b["du"]) <= 1e-6 * b["du"] + 1e-14
+    for a, b in zip(st, rst):  # (a converged run's du sits at the round-off level, ~1e-11)
+        assert abs(a["du_rel"] - b["du"]) <= 1e-6 * b["du"] + 1e-12
     return st, rst
 
 
