@@ -11,6 +11,10 @@
 
 namespace anb {
 
+// Reverse Cuthill-McKee order of the cell graph: per connected component, a pseudo-peripheral
+// start (up to four BFS sweeps, each restarted from the last level's lowest-degree node), then a
+// BFS that appends each node's unvisited neighbours by ascending (degree, index); the whole order
+// reversed.  Queues are flat arrays (the order itself for the final BFS).
 std::vector<int> rcm_order(int n, const std::vector<int>& off, const std::vector<int>& adj) {
   std::vector<int> deg(n);
   for (int i = 0; i < n; ++i) deg[i] = off[i + 1] - off[i];
@@ -18,61 +22,66 @@ std::vector<int> rcm_order(int n, const std::vector<int>& off, const std::vector
   order.reserve(n);
   std::vector<char> seen(n, 0);
   std::vector<int> level(n, -1);
-  auto bfs_last = [&](int s, int& depth) {  // returns a node of the last BFS level with min degree
-    std::vector<int> q{s};
-    std::vector<int> touched{s};
+  std::vector<int> q;
+  q.reserve(n);
+  // BFS from s; returns the lowest-degree node (first met) of the last level, depth = its level
+  auto bfs_last = [&](int s, int& depth) {
+    q.clear();
+    q.push_back(s);
     level[s] = 0;
-    size_t h = 0;
     int last = s;
     depth = 0;
-    while (h < q.size()) {
-      int v = q[h++];
+    for (size_t h = 0; h < q.size(); ++h) {
+      const int v = q[h];
       if (level[v] > depth || (level[v] == depth && deg[v] < deg[last])) {
         depth = level[v];
         last = v;
       }
       for (int k = off[v]; k < off[v + 1]; ++k) {
-        int w = adj[k];
+        const int w = adj[k];
         if (level[w] < 0) {
           level[w] = level[v] + 1;
           q.push_back(w);
-          touched.push_back(w);
         }
       }
     }
-    for (int v : touched) level[v] = -1;
+    for (int v : q) level[v] = -1;
     return last;
   };
   std::vector<int> nb;
   for (int s0 = 0; s0 < n; ++s0) {
     if (seen[s0]) continue;
-    // pseudo-peripheral start: a few BFS sweeps from a min-degree node of the component
     int s = s0, d0 = -1;
     for (int it = 0; it < 4; ++it) {
       int d;
-      int t = bfs_last(s, d);
+      const int t = bfs_last(s, d);
       if (d <= d0) break;
       d0 = d;
       s = t;
     }
-    std::vector<int> comp;
-    std::queue<int> q;
-    q.push(s);
+    size_t h = order.size();
+    order.push_back(s);
     seen[s] = 1;
-    while (!q.empty()) {
-      int v = q.front();
-      q.pop();
-      comp.push_back(v);
+    while (h < order.size()) {
+      const int v = order[h++];
       nb.clear();
       for (int k = off[v]; k < off[v + 1]; ++k)
         if (!seen[adj[k]]) nb.push_back(adj[k]);
-      std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+      // insertion sort by (degree, index): the lists are a handful of entries
+      for (size_t i = 1; i < nb.size(); ++i) {
+        const int x = nb[i];
+        size_t j = i;
+        while (j > 0 && (deg[nb[j - 1]] > deg[x] || (deg[nb[j - 1]] == deg[x] && nb[j - 1] > x))) {
+          nb[j] = nb[j - 1];
+          --j;
+        }
+        nb[j] = x;
+      }
       for (int w : nb) {
         seen[w] = 1;
-        q.push(w);
+        order.push_back(w);
       }
     }
-    order.insert(order.end(), comp.begin(), comp.end());
   }
   std::reverse(order.begin(), order.end());
   return order;
