@@ -44,7 +44,8 @@ class Params(ct.Structure):
                 ("vel_maxit", ct.c_int), ("vel_tol", ct.c_double), ("vel_rel_tol", ct.c_double),
                 ("p_maxit", ct.c_int), ("p_tol", ct.c_double), ("p_rel_tol", ct.c_double),
                 ("corr_tol", ct.c_double), ("p_amg_rebuild_every", ct.c_int), ("p_use_amg", ct.c_int),
-                ("precision", ct.c_int), ("device", ct.c_int), ("p_amg_setup_scope", ct.c_int)]
+                ("precision", ct.c_int), ("device", ct.c_int), ("p_amg_setup_scope", ct.c_int),
+                ("mom_amg", ct.c_int)]
 
 
 class IterStats(ct.Structure):

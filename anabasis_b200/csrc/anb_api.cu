@@ -113,6 +113,13 @@ void poll(anb_ctx* c, const int* dflags, int count) {
 void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3]);
 void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv);
 
+// Right preconditioner of the momentum BiCGSTAB with mom_amg: one V-cycle of the momentum
+// hierarchy for component q after the p update (which = 0) or the s update (which = 1).
+void mom_apply(void* ctx, int q, int which) {
+  anb_ctx* c = static_cast<anb_ctx*>(ctx);
+  amg_apply(c->lc, c->momArgs[2 * q + which], &c->amgMom, &c->momGraph[2 * q + which]);
+}
+
 void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
   ProfScope whole(c->lc, kKfMomentumSolve, 0.0, 0);
   if (c->mixed) return solve_momentum_mixed(c, active, its, conv);
@@ -129,6 +136,7 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
   a.rtol = c->prm.vel_rel_tol;
   a.maxit = c->prm.vel_maxit;
   a.red = c->red;
+  a.precond = (c->prm.mom_amg && c->momAmgBuilt && c->amgMom.nLevels >= 2) ? 1 : 0;
   bicg_init(c->lc, a);
   // freeze inactive components
   for (int q = 0; q < 3; ++q)
@@ -139,7 +147,10 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
   int done = 0;
   int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
   while (true) {
-    for (int k = 0; k < batch; ++k) bicg_iteration(c->lc, a);
+    for (int k = 0; k < batch; ++k) {
+      if (a.precond) bicg_iteration_precond(c->lc, a, mom_apply, c);
+      else bicg_iteration(c->lc, a);
+    }
     done += batch;
     poll(c, a.fl, 12);
     bool all = true;
@@ -248,9 +259,11 @@ constexpr int kAmgFusedDownRows = 65536;
 constexpr int kBlocksPerSM = 8;
 
 // Aggregation hierarchy for the current level-0 matrix (val0/diag0 on the device, storage type T),
-// coarse levels in T, coarsest inverse in double; the V-cycle is captured as a graph for `ga`.
+// coarse levels in T, coarsest inverse in double, host structure in H, device arrays in ar.  For the
+// pressure hierarchy (ga != nullptr) the PCG V-cycles are captured as graphs for *ga.
 template <class T>
-void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const PcgArgsT<T>& ga) {
+void build_amg(anb_ctx* c, AmgDevT<T>& A, std::vector<AmgLevelHost>& H, DevArena& ar, T* val0, T* diag0, T* wdinv0,
+               const PcgArgsT<T>* ga) {
   std::vector<T> hv(c->nEnt), hd(c->C);
   CK(cudaMemcpyAsync(hv.data(), val0, hv.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(hd.data(), diag0, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
@@ -264,12 +277,11 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
       if (*q == ',') ++q;
     }
   }
-  c->amgHost = build_amg_hierarchy(c->L, std::vector<double>(hv.begin(), hv.end()),
+  H = build_amg_hierarchy(c->L, std::vector<double>(hv.begin(), hv.end()),
                                    std::vector<double>(hd.begin(), hd.end()), opt);
-  A.nLevels = (int)c->amgHost.size();
-  DevArena& ar = c->amgArena;
+  A.nLevels = (int)H.size();
   for (int l = 0; l < A.nLevels; ++l) {
-    const AmgLevelHost& h = c->amgHost[l];
+    const AmgLevelHost& h = H[l];
     AmgLevelDevT<T>& d = A.lv[l];
     d = AmgLevelDevT<T>{};
     d.n = h.n;
@@ -302,14 +314,14 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
       d.mem = ar.upload(h.mem);
       d.gOff = ar.upload(h.gOff);
       d.gIdx = ar.upload(h.gIdx);
-      d.nEntNext = c->amgHost[l + 1].nStore;
+      d.nEntNext = H[l + 1].nStore;
     }
   }
-  const int nd = c->amgHost.back().n;
+  const int nd = H.back().n;
   if (nd > 160) throw AnbError(ANB_ERR_UNSUPPORTED, "AMG coarsest level too large (" + std::to_string(nd) + ")");
   A.nDense = nd;
   A.dense = ar.alloc<double>((size_t)nd * nd);
-  c->amgBuilt = true;
+  if (ga) c->amgBuilt = true;
   const char* tailEnv = std::getenv("ANB_AMG_TAIL_ROWS");
   amg_configure_tail(A, tailEnv ? std::atoi(tailEnv) : kAmgTailRows, c->stream);
   const char* fdEnv = std::getenv("ANB_AMG_FUSED_DOWN_ROWS");
@@ -321,18 +333,51 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, T* val0, T* diag0, T* wdinv0, const Pc
     std::fprintf(stderr, " | tail rows %d, cluster %d\n", A.tailRows, A.tailCluster);
   }
   const char* noGraph = std::getenv("ANB_NO_GRAPH");
-  if (A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) CK(amg_capture_graph(c->lc, ga, A));
+  if (ga && A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) CK(amg_capture_graph(c->lc, *ga, A));
+}
+
+// Momentum AMG (mom_amg): Jacobi weights of the freshly assembled matrix, the hierarchy on first
+// use (its structure is kept; every full assembly refreshes the coarse values), and the arguments
+// of the six V-cycle applications (component q, on p or on s) of the preconditioned BiCGSTAB.
+void mom_amg_refresh(anb_ctx* c) {
+  launch_jacobi_weights(c->lc, c->C, c->amgMom.omega, c->mdiag, c->mwdinv);
+  if (!c->momAmgBuilt) {
+    build_amg<double>(c, c->amgMom, c->amgMomHost, c->amgMomArena, c->mval, c->mdiag, c->mwdinv, nullptr);
+    c->momAmgBuilt = true;
+    const size_t C = c->C;
+    for (int q = 0; q < 3; ++q)
+      for (int which = 0; which < 2; ++which) {
+        PcgArgs& m = c->momArgs[2 * q + which];
+        m = PcgArgs{};
+        m.A = mom_sell(c);
+        m.mode = 1;
+        m.r = (which ? c->bw[4] : c->bw[2]) + q * C;  // s or p of component q
+        m.z = (which ? c->bw[7] : c->bw[6]) + q * C;  // sh or ph
+        m.b = m.r;
+        m.r2 = c->momScratch;
+        m.x = m.q = m.p0 = m.p1 = c->momScratch;    // not read in mode 1
+        m.fl = c->flags + kFlagBicg + 4 * q;          // the component's done flag
+        m.sc = c->momSc;
+        m.red = c->red;
+      }
+  }
+  if (c->amgMom.nLevels >= 2) amg_refresh(c->lc, c->amgMom);
 }
 
 void ensure_amg(anb_ctx* c) {
   if (!c->prm.p_use_amg) return;
   if (c->mixed) {
-    if (!c->amgBuilt)
-      build_amg<float>(c, c->amg32, c->pval32, c->pdiag32, c->pwdinv32, pcg_args32(c, c->r32, c->dx32, 0.0, 0.0));
+    if (!c->amgBuilt) {
+      const PcgArgsT<float> ga = pcg_args32(c, c->r32, c->dx32, 0.0, 0.0);
+      build_amg<float>(c, c->amg32, c->amgHost, c->amgArena, c->pval32, c->pdiag32, c->pwdinv32, &ga);
+    }
     if (c->amg32.nLevels >= 2) amg_refresh(c->lc, c->amg32);
     return;
   }
-  if (!c->amgBuilt) build_amg<double>(c, c->amg, c->pval, c->pdiag, c->pwdinv, pcg_args(c, c->pb, 0.0));
+  if (!c->amgBuilt) {
+    const PcgArgs ga = pcg_args(c, c->pb, 0.0);
+    build_amg<double>(c, c->amg, c->amgHost, c->amgArena, c->pval, c->pdiag, c->pwdinv, &ga);
+  }
   if (c->amg.nLevels >= 2) amg_refresh(c->lc, c->amg);
 }
 
@@ -539,6 +584,7 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   }
   // 2. momentum matrix (u pass) + three right-hand sides + relaxation + rAU
   launch_mom(c, c->U, 0);
+  if (p.mom_amg) mom_amg_refresh(c);
   CK(cudaMemcpyAsync(c->Us, c->U, sizeof(double) * 3 * C, cudaMemcpyDeviceToDevice, c->stream));
   int its[3] = {0, 0, 0};
   {
@@ -881,6 +927,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     dm.sliceOff = A.upload(L.sliceOff);
     dm.col = A.upload(L.col);
     dm.slotFace = A.upload(L.slotFace);
+    dm.fOwner = A.upload(L.fOwner);
+    dm.fNeigh = A.upload(L.fNeigh);
     dm.face = c->dFace;
     dm.fFlags = A.upload(L.fFlags);
     {
@@ -971,6 +1019,13 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     }
     c->pdx = A.alloc<double>(C);
     if (prm->n_vel_nonorth_corr > 0) c->UsPrev = A.alloc<double>(3 * C);
+    if (prm->mom_amg) {
+      if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "mom_amg needs an FP64 context");
+      c->mwdinv = A.alloc<double>(C);
+      c->momScratch = A.alloc<double>(C);
+      c->momSc = A.alloc<double>(8);
+      c->amgMom.corr = 1.0;
+    }
     if (prm->p_amg_setup_scope != 0 && prm->p_amg_setup_scope != 1)
       throw AnbError(ANB_ERR_INVALID, "p_amg_setup_scope must be 0 (outer) or 1 (pressure)");
     if (const char* s = std::getenv("ANB_AMG_OMEGA")) c->amg.omega = std::atof(s);
@@ -1017,6 +1072,8 @@ void anb_destroy(anb_ctx* c) {
   for (auto g : c->amg.graph)
     if (g) cudaGraphExecDestroy(g);
   for (auto g : c->amg32.graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto g : c->momGraph)
     if (g) cudaGraphExecDestroy(g);
   adjoint_release(c);
   c->amgArena.release();

@@ -136,6 +136,15 @@ struct anb_ctx {
   anb::AdjointData* adj = nullptr;
   // anb_create wall seconds: copy-in + topology, geometry, layout, device build + upload
   double setupSec[4] = {0, 0, 0, 0};
+  // momentum AMG preconditioner (mom_amg = 1): hierarchy of the momentum matrix, level-0 Jacobi
+  // weights, V-cycle arguments and graphs per (component, p or s) application, scratch vector
+  bool momAmgBuilt = false;
+  AmgDev amgMom;
+  std::vector<AmgLevelHost> amgMomHost;
+  DevArena amgMomArena;
+  double *mwdinv = nullptr, *momScratch = nullptr, *momSc = nullptr;
+  PcgArgs momArgs[6] = {};
+  cudaGraphExec_t momGraph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace anb {

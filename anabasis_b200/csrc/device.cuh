@@ -32,6 +32,8 @@ struct DMesh {
   const int* sliceOff;
   const int* col;
   const int* slotFace;
+  const int* fOwner;    // internal faces in layout order: owner (lower new index) and neighbour
+  const int* fNeigh;
   const FaceRec* face;
   const uint8_t* fFlags;
   // the face record of every slot, copied into slot order as 8 arrays of nEnt doubles (lam, g,

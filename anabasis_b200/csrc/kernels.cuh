@@ -220,6 +220,8 @@ struct BicgArgsT {
   double atol, rtol;
   int maxit;
   Reducer red;
+  int precond;        // 0: Jacobi (ph = D^-1 p, sh = D^-1 s in the vector kernels); 1: the caller
+                      // applies its preconditioner to p and s (bicg_iteration_precond)
 };
 using BicgArgs = BicgArgsT<double>;
 template <class T>
@@ -237,6 +239,8 @@ struct PcgArgsT {
   // down sweep applies r_new = r - alpha q and x += alpha p itself, reading the old residual of
   // the neighbour rows from one buffer while it writes the new one into the other.
   T* r2;
+  int mode;           // 0: PCG iteration; 1: plain preconditioner application z = M^-1 r (no update of
+                      // x or r, no r.z reduction; fl[0] is the caller's done flag)
   double* sc;         // rz, alpha, beta, eps, rr, pq
   int* fl;            // done, iters, converged, first
   double atol, rtol;
@@ -305,6 +309,15 @@ template <class T>
 void pcg_precondition(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg);
 template <class T>
 void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg);  // Galerkin values + dense inverse
+// z = M^-1 r with one V-cycle for arguments in mode 1 (r input, r2 scratch, z output, fl[0] a done
+// flag that skips the application); captured into *graph on the first call when graph != nullptr
+template <class T>
+void amg_apply(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg, cudaGraphExec_t* graph);
+// One BiCGSTAB iteration with an external preconditioner: ph_c = M^-1 p_c after the p update and
+// sh_c = M^-1 s_c after the s update, by apply(c, 0) and apply(c, 1) for the active components
+template <class T>
+void bicg_iteration_precond(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(void* ctx, int c, int which),
+                            void* ctx);
 template <class T>
 cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg);
 // Sets the coarse tail (levels of at most tailRows rows on one cluster; 0 = off) and picks its
@@ -330,6 +343,8 @@ struct DefectArgs {
 void launch_defect(const LaunchCfg& lc, const DefectArgs& a);
 // x += dx (nc*n), dx = 0
 void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, float* dx);
+// wdinv = omega / diag (n rows)
+void launch_jacobi_weights(const LaunchCfg& lc, int n, double omega, const double* diag, double* wdinv);
 
 // ---- steady residual, tangent and adjoint (kernels_adjoint.cu) -----------------------------
 struct AdjArgs {

@@ -5,6 +5,9 @@
 // faces, and accumulates diagonal, right-hand side and divergence in registers.  Each row writes
 // only its own outputs, so the reference's FP64 atomicAdd scatters (main.cu:56-58) become
 // deterministic gathers; a face's flux is written by its owner row.
+#include <cstdlib>
+#include <string>
+
 #include "kernels.cuh"
 
 namespace anb {
@@ -485,6 +488,101 @@ __global__ void __launch_bounds__(kBlock) k_flux_final(DMesh m, FluxArgs a) {
     for (int q = 0; q < 9; ++q) a.stats[q] = acc[q];
 }
 
+// ---- flux correction, face-parallel form -------------------------------------------------
+// Each internal face's corrected flux once, in its owner orientation, by one thread (the
+// expression of flux_slot for the owner row), then a row kernel that sums the divergence in slot
+// order from the stored fluxes and applies the updates of k_flux_final.
+__global__ void __launch_bounds__(kBlock) k_flux_faces(DMesh m, FluxArgs a) {
+  const int C = m.nCells;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nInternal; f += gridDim.x * blockDim.x) {
+    const int P = __ldg(&m.fOwner[f]), N = __ldg(&m.fNeigh[f]);
+    double lam, g, t[3], d[3];
+    load_face(m.face, f, lam, g, t, d);
+    const double rP = __ldg(&a.rau[P]), rN = __ldg(&a.rau[N]);
+    const double pP = __ldg(&a.pc[P]), pN = __ldg(&a.pc[N]);
+    const double l1 = 1.0 - lam;
+    const double rAUf = l1 * rP + lam * rN;
+    double phiNO = 0.0;
+    if (__ldg(&m.fFlags[f]) & 2) {
+      const double gx = l1 * __ldg(&a.Gc[P]) + lam * __ldg(&a.Gc[N]);
+      const double gy = l1 * __ldg(&a.Gc[C + P]) + lam * __ldg(&a.Gc[C + N]);
+      const double gz = l1 * __ldg(&a.Gc[2 * C + P]) + lam * __ldg(&a.Gc[2 * C + N]);
+      phiNO = rAUf * (gx * t[0] + gy * t[1] + gz * t[2]);
+    }
+    a.phi[f] = __ldg(&a.phiStar[f]) - g * rAUf * (pN - pP) - phiNO;
+  }
+}
+
+template <int WM>
+__global__ void __launch_bounds__(kBlock) k_flux_cells(DMesh m, FluxArgs a) {
+  __shared__ double sm[9 * 32];
+  const int C = m.nCells, nI = m.nInternal;
+  const double* Gc = a.Gc;
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < C; r += gridDim.x * blockDim.x) {
+    double div = 0.0;
+    const double pcr = __ldg(&a.pc[r]), rAUr = __ldg(&a.rau[r]);
+    const double gr[3] = {__ldg(&Gc[r]), __ldg(&Gc[C + r]), __ldg(&Gc[2 * C + r])};
+    if constexpr (WM > 0) {
+      int fs[WM], cs[WM];
+      slot_regs<WM>(m, r, fs, cs);
+#pragma unroll
+      for (int k = 0; k < WM; ++k) {
+        if (fs[k] < 0) continue;
+        const double ph = a.phi[fs[k]];
+        div += r < cs[k] ? ph : -ph;
+      }
+    } else {
+      int W;
+      const int base = row_base(m, r, W);
+      for (int k = 0; k < W; ++k) {
+        const int e = base + (k << 5);
+        const int f = __ldg(&m.slotFace[e]);
+        if (f < 0) break;
+        const double ph = a.phi[f];
+        div += r < __ldg(&m.col[e]) ? ph : -ph;
+      }
+    }
+    const int j0 = __ldg(&m.cbOff[r]), j1 = __ldg(&m.cbOff[r + 1]);
+    for (int j = j0; j < j1; ++j) {
+      const int bf = __ldg(&m.cbList[j]);
+      const unsigned ty = __ldg(&m.bType[bf]);
+      double phi = a.phiStar[nI + bf];
+      if ((ty & 8u) && (__ldg(&m.bFlags[bf]) & 2)) {
+        const double g = m.bnd[bf].g;
+        const double* t = m.bnd[bf].t;
+        const double phiNO = rAUr * (gr[0] * t[0] + gr[1] * t[1] + gr[2] * t[2]);
+        phi = phi - g * rAUr * (m.bVal[3 * m.nBoundary + bf] - pcr) - phiNO;
+      }
+      div += phi;
+      a.phi[nI + bf] = phi;
+    }
+    a.divCorr[r] = div;
+    if (a.update) {
+      const double pOld = a.P[r];
+      const double pNew = pOld + a.pRelax * pcr;
+      a.P[r] = pNew;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const double uo = a.U[q * C + r];
+        const double un = a.Us[q * C + r] - rAUr * gr[q];
+        a.U[q * C + r] = un;
+        const double dd = un - uo;
+        acc[2 * q] += dd * dd;
+        acc[2 * q + 1] += un * un;
+      }
+      const double dp = pNew - pOld;
+      acc[6] += dp * dp;
+      acc[7] += pNew * pNew;
+      const double ad = fabs(div);
+      acc[8] = (ad == ad) ? fmax(acc[8], ad) : INFINITY;
+    }
+  }
+  if (!a.update) return;
+  if (grid_reduce<9>(acc, 1u << 8, a.red, sm) && threadIdx.x == 0)
+    for (int q = 0; q < 9; ++q) a.stats[q] = acc[q];
+}
+
 // ---- patch force: main.cu:2828-2933 (single block, deterministic order) -------------------
 __global__ void k_patch_force(DMesh m, int b0, int b1, int sign, double mu, const double* bA, const double* bN,
                               const double* U, const double* P, double* out) {
@@ -650,8 +748,18 @@ void launch_nonorth_rhs(const LaunchCfg& lc, const DMesh& m, const NonOrthArgs& 
   else k_nonorth_rhs<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
 void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a) {
-  ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0);
+  const char* form = std::getenv("ANB_FLUX_FORM");  // "face": the face-parallel form (once per step)
+  const bool faceForm = form && std::string(form) == "face";
   const int wc = sell_width_class(m.maxW);
+  if (faceForm) {
+    ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0, 2);
+    k_flux_faces<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+    if (wc == 4) k_flux_cells<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+    else if (wc == 8) k_flux_cells<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+    else k_flux_cells<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+    return;
+  }
+  ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0);
   if (wc == 4) k_flux_final<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else if (wc == 8) k_flux_final<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else k_flux_final<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);

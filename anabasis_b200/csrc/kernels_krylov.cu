@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgsT<T> a) {
       const size_t i = (size_t)c * n + r;
       const double pn = (double)a.r[i] + beta[c] * ((double)a.p[i] - om[c] * (double)a.v[i]);
       a.p[i] = (T)pn;
-      a.ph[i] = (T)(dinv * pn);
+      if (!a.precond) a.ph[i] = (T)(dinv * pn);
     }
   }
 }
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgsT<T> a) {
       const size_t i = (size_t)c * n + r;
       const double sv = (double)a.r[i] - al[c] * (double)a.v[i];
       a.s[i] = (T)sv;
-      a.sh[i] = (T)(dinv * sv);
+      if (!a.precond) a.sh[i] = (T)(dinv * sv);
       acc[c] += sv * sv;
     }
   }
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid0(PcgArgsT<T> a, AmgLevelDe
                                                        const T* p) {
   __shared__ double sm[32];
   if (a.fl[0]) return;
-  const bool upd = a.fl[3] == 0;
+  const bool upd = a.mode == 0 && a.fl[3] == 0;
   const double al = upd ? a.sc[1] : 0.0;
   double acc[1] = {0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < f.n; i += gridDim.x * blockDim.x) {
@@ -756,7 +756,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
     out[i] = xn;
     if (finest) acc[0] += bi * (double)xn;
   }
-  if (!finest) return;
+  if (!finest || a.mode != 0) return;
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
     const double rzOld = a.sc[0];
     a.sc[2] = a.fl[3] ? 0.0 : acc[0] / rzOld;
@@ -971,6 +971,11 @@ __global__ void __launch_bounds__(kBlock) k_defect(DefectArgs a) {
   }
 }
 
+// wdinv = omega / diag (weighted-Jacobi smoother weights of a level-0 matrix)
+__global__ void __launch_bounds__(kBlock) k_jacobi_weights(int n, double omega, const double* diag, double* wdinv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) wdinv[i] = omega / diag[i];
+}
+
 __global__ void __launch_bounds__(kBlock) k_apply_correction(size_t n, double* x, float* dx) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     x[i] += (double)dx[i];
@@ -985,13 +990,17 @@ void bicg_init(const LaunchCfg& lc, const BicgArgsT<T>& a) {
   g_launches += 1;
   k_bicg_init<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
+// One BiCGSTAB iteration; apply (when given) is the right preconditioner of the active
+// components after the p and the s updates (the vector kernels then leave ph and sh to it).
 template <class T>
-void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
+static void bicg_step(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(void*, int, int), void* ctx) {
   const double vbytes = lc.ab ? lc.ab->bicg_spmv(a.nc) * (sizeof(T) == 4 ? 0.5 : 1.0) : 0.0;
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
     k_bicg_p<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
+  if (apply)
+    for (int c = 0; c < a.nc; ++c) apply(ctx, c, 0);
   const int wc = sell_width_class(a.A.maxW);
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
@@ -1003,6 +1012,8 @@ void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
     ProfScope ps(lc, kKfBicgVector, 0.0);
     k_bicg_s<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
+  if (apply)
+    for (int c = 0; c < a.nc; ++c) apply(ctx, c, 1);
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
     if (wc == 4) k_bicg_t<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
@@ -1013,6 +1024,14 @@ void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
     ProfScope ps(lc, kKfBicgVector, 0.0);
     k_bicg_x<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
+}
+template <class T>
+void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a) {
+  bicg_step(lc, a, nullptr, nullptr);
+}
+template <class T>
+void bicg_iteration_precond(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(void*, int, int), void* ctx) {
+  bicg_step(lc, a, apply, ctx);
 }
 
 template <class T>
@@ -1244,6 +1263,29 @@ void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgD
 }
 
 template <class T>
+void amg_apply(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg, cudaGraphExec_t* graph) {
+  if (graph && !*graph) {
+    LaunchCfg quiet = lc;
+    quiet.prof = nullptr;
+    const long long before = g_launches.load();
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(lc.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      vcycle(quiet, a, amg, 0);
+      const cudaError_t e = cudaStreamEndCapture(lc.stream, &g);
+      if (e == cudaSuccess && cudaGraphInstantiate(graph, g, 0) != cudaSuccess) *graph = nullptr;
+      if (g) cudaGraphDestroy(g);
+    }
+    g_launches = before;
+  }
+  if (graph && *graph) {
+    g_launches += amg->graphKernels;
+    cudaGraphLaunch(*graph, lc.stream);
+  } else {
+    vcycle(lc, a, amg, 0);
+  }
+}
+
+template <class T>
 void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg) {
   for (int l = 0; l + 1 < amg.nLevels; ++l) {
     AmgLevelDevT<T>& f = amg.lv[l];
@@ -1272,6 +1314,11 @@ void launch_defect(const LaunchCfg& lc, const DefectArgs& a) {
   k_defect<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
 
+void launch_jacobi_weights(const LaunchCfg& lc, int n, double omega, const double* diag, double* wdinv) {
+  g_launches += 1;
+  k_jacobi_weights<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(n, omega, diag, wdinv);
+}
+
 void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, float* dx) {
   g_launches += 1;
   k_apply_correction<<<lc.rowBlocks, kBlock, 0, lc.stream>>>((size_t)n * nc, x, dx);
@@ -1285,7 +1332,9 @@ void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, floa
   template void pcg_precondition<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*);  \
   template void amg_refresh<T>(const LaunchCfg&, AmgDevT<T>&);                                \
   template cudaError_t amg_capture_graph<T>(const LaunchCfg&, const PcgArgsT<T>&, AmgDevT<T>&);           \
-  template void amg_configure_tail<T>(AmgDevT<T>&, int, cudaStream_t);
+  template void amg_configure_tail<T>(AmgDevT<T>&, int, cudaStream_t);                          \
+  template void amg_apply<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*, cudaGraphExec_t*); \
+  template void bicg_iteration_precond<T>(const LaunchCfg&, const BicgArgsT<T>&, void (*)(void*, int, int), void*);
 ANB_INSTANTIATE(double)
 ANB_INSTANTIATE(float)
 #undef ANB_INSTANTIATE

@@ -72,6 +72,9 @@ typedef struct anb_params {
   int device;
   int p_amg_setup_scope;     /* pAmgSetupScope (main.cu:89, 2594-2598): 0 refresh the pressure
                                 preconditioner at the rebuild cadence, 1 before every pressure solve */
+  int mom_amg;               /* momentum BiCGSTAB preconditioner: 0 Jacobi (the reference's DiagScale,
+                                main.cu:2553-2576), 1 aggregation AMG V-cycle on the momentum matrix
+                                (FP64 contexts) */
 } anb_params;
 
 /* Per-outer-iteration monitor values (the stdout line of main.cu:3609-3611). */

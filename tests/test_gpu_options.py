@@ -5,6 +5,9 @@
 * nVelNonOrthCorr (main.cu:3350-3384): momentum re-solves with the right-hand side re-assembled
   on the current iterate until the relative change drops below corrTol; the relative change is a
   device reduction.
+* mom_amg: the momentum BiCGSTAB preconditioned by an aggregation-AMG V-cycle of the momentum
+  matrix instead of Jacobi (the reference's DiagScale, main.cu:2553-2576); same fields at the
+  tight tolerances, fewer iterations.
 * pAmgSetupScope pressure (main.cu:2594-2598): the preconditioner is refreshed before every
   pressure solve.  The fine matrix does not change within a step, so the fields equal those of the
   per-step refresh bit for bit, whatever pAmgRebuildEvery says.
@@ -40,7 +43,8 @@ def _run_both(steps, **opts):
 
 @pytest.mark.parametrize("opts", [dict(n_pressure_corr=1), dict(n_pressure_corr=2, n_nonorth_corr=1),
                                   dict(n_vel_nonorth_corr=2, corr_tol=1e-30),
-                                  dict(n_vel_nonorth_corr=3, corr_tol=1e-3, n_pressure_corr=1)])
+                                  dict(n_vel_nonorth_corr=3, corr_tol=1e-3, n_pressure_corr=1),
+                                  dict(mom_amg=1), dict(mom_amg=1, n_vel_nonorth_corr=2, corr_tol=1e-30)])
 def test_options_against_oracle(opts):
     g, st, ref, rst = _run_both(8, **opts)
     assert len(st) == len(rst) == 8
@@ -68,3 +72,21 @@ def test_amg_setup_scope_rejects_unknown():
     m, bc, _ = channel(6, 4, 4)
     with pytest.raises(anb.AnbError):
         anb.Solver(m, anb.default_params(**PRM, p_amg_setup_scope=2))
+
+
+def test_momentum_amg_needs_fewer_iterations():
+    m, bc, _ = channel(**MESH)
+    its = {}
+    for amg in (0, 1):
+        s = anb.Solver(m, anb.default_params(**PRM, mom_amg=amg))
+        s.set_bc(bc)
+        s.set_state(*initial_state(m, bc))
+        _, st = s.iterate(5)
+        its[amg] = sum(x["its_u"] + x["its_v"] + x["its_w"] for x in st)
+    assert its[1] < its[0], its
+
+
+def test_momentum_amg_rejected_in_mixed_precision():
+    m, bc, _ = channel(6, 4, 4)
+    with pytest.raises(anb.AnbError):
+        anb.Solver(m, anb.default_params(**PRM, mom_amg=1, precision=1))
