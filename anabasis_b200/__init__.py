@@ -45,7 +45,7 @@ class Params(ct.Structure):
                 ("p_maxit", ct.c_int), ("p_tol", ct.c_double), ("p_rel_tol", ct.c_double),
                 ("corr_tol", ct.c_double), ("p_amg_rebuild_every", ct.c_int), ("p_use_amg", ct.c_int),
                 ("precision", ct.c_int), ("device", ct.c_int), ("p_amg_setup_scope", ct.c_int),
-                ("mom_amg", ct.c_int)]
+                ("mom_amg", ct.c_int), ("mixed_refine", ct.c_int), ("mixed_inner_rtol", ct.c_double)]
 
 
 class IterStats(ct.Structure):

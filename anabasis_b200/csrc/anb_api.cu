@@ -461,6 +461,10 @@ void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3
     }
     c->lastMomIts = std::max(1, mx);
     launch_apply_correction(c->lc, C, 3, c->Us, c->dx32);
+    if (c->prm.mixed_refine == 1) {  // one inner solve per step: the SIMPLE iteration refines
+      for (int q = 0; q < 3; ++q) outerConv[q] = true;
+      break;
+    }
   }
   for (int q = 0; q < 3; ++q) {
     its[q] = active[q] ? tot[q] : 0;
@@ -511,6 +515,10 @@ void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, i
       c->prof.launches -= it - n;
     }
     launch_apply_correction(c->lc, c->C, 1, x, c->dx32);
+    if (c->prm.mixed_refine == 1) {  // one inner solve per step: the SIMPLE iteration refines
+      ok = true;
+      break;
+    }
   }
   *its = tot;
   *conv = ok;
@@ -780,6 +788,8 @@ void anb_default_params(anb_params* p) {
   p->p_use_amg = 1;
   p->precision = ANB_PRECISION_FP64;
   p->device = 0;
+  p->mixed_refine = 0;
+  p->mixed_inner_rtol = 1e-4;
 }
 
 const char* anb_last_error(const anb_ctx* c) { return c ? c->err.c_str() : g_createError.c_str(); }
@@ -998,7 +1008,10 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       CK(cudaMemset(c->mval32, 0, sizeof(float) * c->nEnt));
       CK(cudaMemset(c->pval32, 0, sizeof(float) * c->nEnt));
       CK(cudaMemset(c->dx32, 0, sizeof(float) * 3 * C));
+      c->innerRtol = prm->mixed_inner_rtol > 0.0 ? prm->mixed_inner_rtol : 1e-4;
       if (const char* s = std::getenv("ANB_MIXED_INNER_RTOL")) c->innerRtol = std::atof(s);
+      if (prm->mixed_refine != 0 && prm->mixed_refine != 1)
+        throw AnbError(ANB_ERR_INVALID, "mixed_refine must be 0 or 1");
     }
     c->rhs = A.alloc<double>(3 * C);
     c->pb = A.alloc<double>(C);

@@ -75,6 +75,12 @@ typedef struct anb_params {
   int mom_amg;               /* momentum BiCGSTAB preconditioner: 0 Jacobi (the reference's DiagScale,
                                 main.cu:2553-2576), 1 aggregation AMG V-cycle on the momentum matrix
                                 (FP64 contexts) */
+  int mixed_refine;          /* ANB_PRECISION_MIXED only.  0: every linear solve is an FP64 defect
+                                correction repeated until the plain method's tolerance is met;
+                                1: one FP32 inner solve per system and outer step, to the relative
+                                reduction mixed_inner_rtol, the SIMPLE iteration (FP64 assembly
+                                residuals, fluxes and continuity) being the refinement loop */
+  double mixed_inner_rtol;   /* relative reduction of one FP32 inner solve (default 1e-4) */
 } anb_params;
 
 /* Per-outer-iteration monitor values (the stdout line of main.cu:3609-3611). */
