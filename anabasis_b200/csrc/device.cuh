@@ -104,7 +104,9 @@ using DSell = DSellT<double>;
 
 // Kernels specialised on a compile-time row width WM hold a row's slots in registers; this picks
 // the smallest specialisation that covers the matrix (0: the generic loop).
-__host__ __device__ inline int sell_width_class(int maxW) { return maxW <= 0 ? 0 : maxW <= 4 ? 4 : maxW <= 8 ? 8 : 0; }
+__host__ __device__ inline int sell_width_class(int maxW) {
+  return maxW <= 0 ? 0 : maxW <= 4 ? 4 : maxW <= 6 ? 6 : maxW <= 8 ? 8 : 0;
+}
 
 // Cross-block deterministic reductions: each block writes a partial, the last block to arrive
 // (atomic ticket) combines the partials in block order.

@@ -720,6 +720,7 @@ void launch_lsq_grad(const LaunchCfg& lc, const DMesh& m, const GradArgs& a) {
   ProfScope ps(lc, kKfGradient, lc.ab ? lc.ab->gradient(a.nf) : 0.0);
   const int wc = sell_width_class(m.maxW);
   if (wc == 4) lsq_grad_w<4>(lc, m, a);
+  else if (wc == 6) lsq_grad_w<6>(lc, m, a);
   else if (wc == 8) lsq_grad_w<8>(lc, m, a);
   else lsq_grad_w<0>(lc, m, a);
 }
@@ -728,6 +729,7 @@ void launch_momentum(const LaunchCfg& lc, const DMesh& m, const MomArgsT<M>& a) 
   ProfScope ps(lc, kKfMomentum, lc.ab ? lc.ab->momentum() : 0.0);
   const int wc = sell_width_class(m.maxW);
   if (wc == 4) k_momentum<M, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 6) k_momentum<M, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else if (wc == 8) k_momentum<M, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else k_momentum<M, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
@@ -744,6 +746,7 @@ void launch_nonorth_rhs(const LaunchCfg& lc, const DMesh& m, const NonOrthArgs& 
   ProfScope ps(lc, kKfNonOrth, lc.ab ? lc.ab->nonorth() : 0.0);
   const int wc = sell_width_class(m.maxW);
   if (wc == 4) k_nonorth_rhs<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 6) k_nonorth_rhs<6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else if (wc == 8) k_nonorth_rhs<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else k_nonorth_rhs<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }
@@ -755,12 +758,14 @@ void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a) {
     ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0, 2);
     k_flux_faces<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
     if (wc == 4) k_flux_cells<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+    else if (wc == 6) k_flux_cells<6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
     else if (wc == 8) k_flux_cells<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
     else k_flux_cells<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
     return;
   }
   ProfScope ps(lc, kKfFluxFinal, lc.ab ? lc.ab->flux_final() : 0.0);
   if (wc == 4) k_flux_final<4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
+  else if (wc == 6) k_flux_final<6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else if (wc == 8) k_flux_final<8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
   else k_flux_final<0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(m, a);
 }

@@ -1005,6 +1005,7 @@ static void bicg_step(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
     if (wc == 4) k_bicg_v<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    else if (wc == 6) k_bicg_v<T, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
     else if (wc == 8) k_bicg_v<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
     else k_bicg_v<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
@@ -1017,6 +1018,7 @@ static void bicg_step(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
     if (wc == 4) k_bicg_t<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    else if (wc == 6) k_bicg_t<T, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
     else if (wc == 8) k_bicg_t<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
     else k_bicg_t<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
   }
@@ -1119,6 +1121,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     const int wc = sell_width_class(f.maxW);
     const int nb = blocks_for(f.n, lc.rowBlocks);
     if (wc == 4) k_amg_resid0<T, 4><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
+    else if (wc == 6) k_amg_resid0<T, 6><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
     else if (wc == 8) k_amg_resid0<T, 8><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
     else k_amg_resid0<T, 0><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
@@ -1135,6 +1138,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
         const int wc = sell_width_class(f.maxW);
         const int nb = blocks_for(f.n, lc.rowBlocks);
         if (wc == 4) k_amg_resid<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+        else if (wc == 6) k_amg_resid<T, 6><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
         else if (wc == 8) k_amg_resid<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
         else k_amg_resid<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
         k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
@@ -1163,6 +1167,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
         const int wc = sell_width_class(f.maxW);
         const int nb = blocks_for(f.n, lc.rowBlocks);
         if (wc == 4) k_amg_up<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
+        else if (wc == 6) k_amg_up<T, 6><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
         else if (wc == 8) k_amg_up<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
         else k_amg_up<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
         continue;
@@ -1178,6 +1183,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     const int wc = sell_width_class(f.maxW);
     const int nb = blocks_for(f.n, lc.rowBlocks);
     if (wc == 4) k_amg_up<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
+    else if (wc == 6) k_amg_up<T, 6><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
     else if (wc == 8) k_amg_up<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
     else k_amg_up<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
   }
@@ -1246,6 +1252,7 @@ void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgD
     ProfScope ps(lc, kKfPcgSpmv, by);
     const int wc = sell_width_class(a.A.maxW);
     if (wc == 4) k_pcg_pq<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+    else if (wc == 6) k_pcg_pq<T, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
     else if (wc == 8) k_pcg_pq<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
     else k_pcg_pq<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
   }
