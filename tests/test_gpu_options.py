@@ -36,7 +36,7 @@ def _run_both(steps, **opts):
     g = s.get_state()
     o = oracle.Oracle(m.topology())
     o.set_bc(bc)
-    oo = {k: v for k, v in opts.items() if k in ("n_pressure_corr", "n_vel_nonorth_corr", "corr_tol")}
+    oo = {k: v for k, v in opts.items() if k in ("n_pressure_corr", "n_vel_nonorth_corr", "corr_tol", "n_nonorth_corr")}
     ref, rst = o.run(oracle.params(**PRM, **TIGHT, **oo), steps, u0, v0, w0, p0)
     return g, st, ref, rst
 
