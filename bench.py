@@ -306,6 +306,55 @@ def run_reference(args, rank: int, world: int) -> dict | None:
     }
 
 
+def run_variants(args) -> dict:
+    """Design switches on the benchmark workload (FP64, steps 5-14 after 4 warm-up steps, CUDA
+    events): the flux correction's row form against its face-parallel form (ANB_FLUX_FORM), and
+    the momentum BiCGSTAB's Jacobi preconditioner against the momentum AMG (mom_amg)."""
+    import ctypes
+
+    import anabasis_b200 as anb
+
+    m, bc, state = make_case()
+    lib = anb.lib()
+
+    def timed(family, env, **prm):
+        old = {k: os.environ.get(k) for k in env}
+        os.environ.update(env)
+        try:
+            s = anb.Solver(m, anb.default_params(**PARAMS, **prm))
+            s.set_bc(bc)
+            s.set_state(*state)
+            s.iterate(4)
+            lib.anb_profile_select(s._h, family)
+            _, st = s.iterate(10)
+            n = ctypes.c_longlong(0)
+            sec, by = np.zeros(1), np.zeros(1)
+            lib.anb_profile_read(s._h, ctypes.byref(n), sec.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 by.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+            s.close()
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        return dict(step_ms=1e3 * sum(x["iter_seconds"] for x in st) / len(st), family_seconds=float(sec[0]),
+                    family_launches=int(n.value), algo_gbs=float(by[0] / sec[0] / 1e9) if sec[0] > 0 else None,
+                    bicg_its=[st[-1]["its_u"], st[-1]["its_v"], st[-1]["its_w"]])
+
+    out = {"metric": "design switches, FP64 SIMPLE on the benchmark workload", "unit": "ms per step",
+           "config": bench_config(1)}
+    for form in ("row", "face"):
+        r = timed(5, {"ANB_FLUX_FORM": form})
+        r["us_per_flux_call"] = 1e6 * r["family_seconds"] / max(r["family_launches"], 1)
+        out[f"flux_{form}"] = r
+    for amg in (0, 1):
+        r = timed(13, {}, mom_amg=amg)
+        r["momentum_ms_per_step"] = 1e3 * r["family_seconds"] / 10
+        out[f"momentum_{'amg' if amg else 'jacobi'}"] = r
+    return out
+
+
 def run_cpu_baselines(args) -> dict:
     """The oracle port (C++/OpenMP, all host threads, Jacobi-PCG / Jacobi-BiCGSTAB at the reference's
     1e-10 tolerances) on configurations 1-3, each case built by the oracle alone: config 1 (16,000
@@ -565,7 +614,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--config", default="obstacle1m",
-                    choices=["obstacle1m", "mixed4m", "adjoint1m", "tets16m", "cpu3"],
+                    choices=["obstacle1m", "mixed4m", "adjoint1m", "tets16m", "cpu3", "variants"],
                     help="obstacle1m: the headline SIMPLE throughput line; the others are single-GPU studies "
                          "of the mixed-precision, adjoint and 16M-tet configurations")
     ap.add_argument("--max-steps", type=int, default=4000)
@@ -579,7 +628,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     studies = {"mixed4m": run_mixed4m, "adjoint1m": run_adjoint1m, "tets16m": run_tets16m,
-               "cpu3": run_cpu_baselines}
+               "cpu3": run_cpu_baselines, "variants": run_variants}
     if args.impl == "reference":
         out = run_reference(args, rank, world)
     elif args.config in studies:
