@@ -328,8 +328,10 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, std::vector<AmgLevelHost>& H, DevArena
   A.fusedDownRows = fdEnv ? std::atoi(fdEnv) : kAmgFusedDownRows;
   const char* verbose = std::getenv("ANB_AMG_VERBOSE");
   if (verbose && verbose[0] == '1') {
-    std::fprintf(stderr, "AMG levels:");
-    for (int l = 0; l < A.nLevels; ++l) std::fprintf(stderr, " %d", A.lv[l].n);
+    std::fprintf(stderr, "AMG levels (rows/stored entries/max width):");
+    for (int l = 0; l < A.nLevels; ++l)
+      std::fprintf(stderr, " %d/%lld/%d", A.lv[l].n, l == 0 ? (long long)c->nEnt : (long long)H[l].nStore,
+                   l == 0 ? c->L.maxRowLen : H[l].maxW);
     std::fprintf(stderr, " | tail rows %d, cluster %d\n", A.tailRows, A.tailCluster);
   }
   const char* noGraph = std::getenv("ANB_NO_GRAPH");
@@ -890,6 +892,10 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       const char* bps = std::getenv("ANB_BLOCKS_PER_SM");
       const int perSM = bps ? std::max(1, std::min(64, std::atoi(bps))) : kBlocksPerSM;
       c->lc.rowBlocks = std::max(1, std::min((c->C + kBlock - 1) / kBlock, nSM * perSM));
+      // the SELL row kernels get one full wave of resident blocks; ANB_GRID=fixed gives every row
+      // kernel rowBlocks blocks instead
+      const char* gp = std::getenv("ANB_GRID");
+      c->lc.nSM = (gp && std::string(gp) == "fixed") ? 0 : nSM;
     }
     c->lc.prof = &c->prof;
     c->lc.ab = &c->ab;

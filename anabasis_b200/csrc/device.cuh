@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdlib>
 #include <cuda_runtime.h>
 
 namespace anb {
@@ -106,6 +107,19 @@ using DSell = DSellT<double>;
 // the smallest specialisation that covers the matrix (0: the generic loop).
 __host__ __device__ inline int sell_width_class(int maxW) {
   return maxW <= 0 ? 0 : maxW <= 4 ? 4 : maxW <= 6 ? 6 : maxW <= 8 ? 8 : 0;
+}
+
+// Width class a launch wrapper instantiates.  ANB_SELL_WIDTH (4, 6 or 8) forces a wider class
+// than the rows need, for measurements; a class narrower than maxW is ignored.  The arithmetic
+// is the same in every class (padding slots are skipped).
+inline int launch_width_class(int maxW) {
+  static const int forced = [] {
+    const char* s = std::getenv("ANB_SELL_WIDTH");
+    return s ? std::atoi(s) : 0;
+  }();
+  const int wc = sell_width_class(maxW);
+  if (wc > 0 && (forced == 4 || forced == 6 || forced == 8) && forced >= maxW) return forced;
+  return wc;
 }
 
 // Cross-block deterministic reductions: each block writes a partial, the last block to arrive

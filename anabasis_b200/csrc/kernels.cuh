@@ -4,6 +4,7 @@
 #include "device.cuh"
 
 #include <atomic>
+#include <type_traits>
 #include <vector>
 
 namespace anb {
@@ -47,11 +48,42 @@ extern std::atomic<long long> g_launches;
 
 struct AlgoBytes;
 struct LaunchCfg {
-  int rowBlocks;   // grid for row-parallel kernels (grid-stride)
+  int rowBlocks;   // most blocks a row-parallel (grid-stride) kernel gets; sizes the reduction partials
   cudaStream_t stream;
   Prof* prof = nullptr;
   const AlgoBytes* ab = nullptr;
+  int nSM = 0;     // > 0: kernels launched through launch_rows get one full wave (see row_grid)
 };
+
+// Blocks of kBlock threads of `kernel` that fit on one SM at once (registers, shared memory);
+// queried once per kernel.
+int resident_blocks(const void* kernel);
+
+// Grid of a grid-stride row kernel: one full wave of its resident blocks on every SM, at most
+// `cap`.  With more blocks than fit, the blocks past the first wave run on a partly idle GPU at the
+// end of the launch; the latency-bound SELL kernels lose up to 10 % to that tail.
+inline int row_grid(const LaunchCfg& lc, const void* kernel, int cap) {
+  if (lc.nSM <= 0) return cap;
+  const int wave = resident_blocks(kernel) * lc.nSM;
+  return wave > 0 && wave < cap ? wave : cap;
+}
+
+template <class... P, class... A>
+inline void launch_rows(const LaunchCfg& lc, int cap, void (*kernel)(P...), A&&... args) {
+  kernel<<<row_grid(lc, (const void*)kernel, cap), kBlock, 0, lc.stream>>>(static_cast<A&&>(args)...);
+}
+
+// Calls fn(std::integral_constant<int, W>) with the width class W (4, 6, 8 or 0 = generic) that a
+// SELL matrix of rows of at most maxW slots is launched with.
+template <class F>
+inline void with_width(int maxW, F&& fn) {
+  switch (launch_width_class(maxW)) {
+    case 4: fn(std::integral_constant<int, 4>{}); break;
+    case 6: fn(std::integral_constant<int, 6>{}); break;
+    case 8: fn(std::integral_constant<int, 8>{}); break;
+    default: fn(std::integral_constant<int, 0>{}); break;
+  }
+}
 
 // Records a start/stop event pair around the launches in its scope when `fam` is selected.
 struct ProfScope {

@@ -1001,13 +1001,9 @@ static void bicg_step(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(
   }
   if (apply)
     for (int c = 0; c < a.nc; ++c) apply(ctx, c, 0);
-  const int wc = sell_width_class(a.A.maxW);
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
-    if (wc == 4) k_bicg_v<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-    else if (wc == 6) k_bicg_v<T, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-    else if (wc == 8) k_bicg_v<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-    else k_bicg_v<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_bicg_v<T, W.value>, a); });
   }
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
@@ -1017,14 +1013,11 @@ static void bicg_step(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(
     for (int c = 0; c < a.nc; ++c) apply(ctx, c, 1);
   {
     ProfScope ps(lc, kKfBicgSpmv, vbytes);
-    if (wc == 4) k_bicg_t<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-    else if (wc == 6) k_bicg_t<T, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-    else if (wc == 8) k_bicg_t<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
-    else k_bicg_t<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_bicg_t<T, W.value>, a); });
   }
   {
     ProfScope ps(lc, kKfBicgVector, 0.0);
-    k_bicg_x<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+    launch_rows(lc, lc.rowBlocks, k_bicg_x<T>, a);
   }
 }
 template <class T>
@@ -1118,12 +1111,8 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
   {
     const AmgLevelDevT<T>& f = f0;
     ProfScope ps(lc, kKfAmgResid0, 0.0, 2);
-    const int wc = sell_width_class(f.maxW);
     const int nb = blocks_for(f.n, lc.rowBlocks);
-    if (wc == 4) k_amg_resid0<T, 4><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
-    else if (wc == 6) k_amg_resid0<T, 6><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
-    else if (wc == 8) k_amg_resid0<T, 8><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
-    else k_amg_resid0<T, 0><<<nb, kBlock, 0, lc.stream>>>(a, f, rIn, rOut, p);
+    with_width(f.maxW, [&](auto W) { launch_rows(lc, nb, k_amg_resid0<T, W.value>, a, f, rIn, rOut, p); });
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
@@ -1135,12 +1124,8 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     for (int l = 1; l < t0; ++l) {
       const AmgLevelDevT<T>& f = amg->lv[l];
       if (f.sliceOff) {  // large coarse level in SELL-32: the level-0 kernels, thread per row
-        const int wc = sell_width_class(f.maxW);
         const int nb = blocks_for(f.n, lc.rowBlocks);
-        if (wc == 4) k_amg_resid<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
-        else if (wc == 6) k_amg_resid<T, 6><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
-        else if (wc == 8) k_amg_resid<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
-        else k_amg_resid<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, amg->omega);
+        with_width(f.maxW, [&](auto W) { launch_rows(lc, nb, k_amg_resid<T, W.value>, a.fl, f, amg->omega); });
         k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
         continue;
       }
@@ -1164,12 +1149,10 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
       // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
       const T* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
       if (f.sliceOff) {
-        const int wc = sell_width_class(f.maxW);
         const int nb = blocks_for(f.n, lc.rowBlocks);
-        if (wc == 4) k_amg_up<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
-        else if (wc == 6) k_amg_up<T, 6><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
-        else if (wc == 8) k_amg_up<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
-        else k_amg_up<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
+        with_width(f.maxW, [&](auto W) {
+          launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
+        });
         continue;
       }
       k_amg_up_csr<kCoarseLanes, T><<<blocks_for(f.n * kCoarseLanes, lc.rowBlocks), kBlock, 0, lc.stream>>>(
@@ -1180,12 +1163,10 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     const AmgLevelDevT<T>& f = f0;
     const T* e = (L == 2) ? amg->lv[1].x : amg->lv[1].x2;
     ProfScope ps(lc, kKfAmgUp0, 0.0);
-    const int wc = sell_width_class(f.maxW);
     const int nb = blocks_for(f.n, lc.rowBlocks);
-    if (wc == 4) k_amg_up<T, 4><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
-    else if (wc == 6) k_amg_up<T, 6><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
-    else if (wc == 8) k_amg_up<T, 8><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
-    else k_amg_up<T, 0><<<nb, kBlock, 0, lc.stream>>>(a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
+    with_width(f.maxW, [&](auto W) {
+      launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
+    });
   }
 }
 
@@ -1250,11 +1231,7 @@ void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgD
     // values and vectors halve in FP32
     const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
     ProfScope ps(lc, kKfPcgSpmv, by);
-    const int wc = sell_width_class(a.A.maxW);
-    if (wc == 4) k_pcg_pq<T, 4><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
-    else if (wc == 6) k_pcg_pq<T, 6><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
-    else if (wc == 8) k_pcg_pq<T, 8><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
-    else k_pcg_pq<T, 0><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a, pOld, pNew);
+    with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, W.value>, a, pOld, pNew); });
   }
   if (useAmg) {
     // the V-cycle's level-0 sweep applies x += alpha pNew, r -= alpha q: variant (it + 1) & 1 reads
