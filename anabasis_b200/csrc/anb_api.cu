@@ -201,17 +201,22 @@ PcgArgs pcg_args(anb_ctx* c, const double* b, double rtol) {
   return a;
 }
 
-// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
-void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
-  ProfScope whole(c->lc, kKfPressureSolve, 0.0, 0);
-  if (c->mixed) return solve_pressure_mixed(c, b, x, rtol, its, conv);
-  PcgArgs a = pcg_args(c, b, rtol);
-  const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
-  CK(cudaMemcpyAsync(c->pxw, x, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
-  pcg_init(c->lc, a);
-  pcg_precondition(c->lc, a, amg);
-  // enqueue most of the expected iterations (previous solve's count) before the first poll,
-  // then poll in small batches; iterations after convergence return at once
+// The PCG iterations after pcg_init + pcg_precondition, until the solve is done: one launch of the
+// hierarchy's loop graph when it holds one for these arguments (and no PCG or V-cycle kernel family
+// is being timed), else batches of pcg_iteration, most of the expected iterations (previous
+// solve's count) before the first poll, then small batches.  Iterations after convergence return
+// at once either way.  Returns the iterations enqueued; hFlags holds the PCG flags afterwards.
+template <class T>
+int pcg_iterate(anb_ctx* c, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
+  const int fam = c->prof.family;
+  const bool timed = fam >= kKfPcgSpmv && fam <= kKfPcgUpdate;
+  if (amg && !timed && pcg_loop_launch(c->lc, a, *amg)) {
+    poll(c, a.fl, 5);
+    const int trips = c->hFlags[4];
+    const int enq = 2 * std::max(trips - 1, 0);
+    g_launches += trips + (long long)enq * (1 + amg->graphKernels);
+    return enq;
+  }
   int it = 0;
   int batch = std::max(2, std::min(3 * c->lastPIts / 4, 64));
   const int tail = std::max(2, c->lastPIts / 8);
@@ -221,6 +226,19 @@ void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* it
     if (c->hFlags[0] || it > a.maxit + 2) break;
     batch = tail;
   }
+  return it;
+}
+
+// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
+void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  ProfScope whole(c->lc, kKfPressureSolve, 0.0, 0);
+  if (c->mixed) return solve_pressure_mixed(c, b, x, rtol, its, conv);
+  PcgArgs a = pcg_args(c, b, rtol);
+  const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
+  CK(cudaMemcpyAsync(c->pxw, x, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
+  pcg_init(c->lc, a);
+  pcg_precondition(c->lc, a, amg);
+  const int it = pcg_iterate(c, a, amg);
   CK(cudaMemcpyAsync(x, c->pxw, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
   *its = c->hFlags[1];
   *conv = c->hFlags[2] != 0;
@@ -500,15 +518,7 @@ void solve_pressure_mixed(anb_ctx* c, const double* b, double* x, double rtol, i
     PcgArgsT<float> a = pcg_args32(c, c->r32, c->dx32, 0.5 * target, c->innerRtol);
     pcg_init(c->lc, a);
     pcg_precondition(c->lc, a, amg);
-    int it = 0;
-    int batch = std::max(2, std::min(3 * c->lastPIts / 4, 64));
-    const int tail = std::max(2, c->lastPIts / 8);
-    while (true) {
-      for (int k = 0; k < batch; ++k) pcg_iteration(c->lc, a, it++, amg);
-      poll(c, a.fl, 4);
-      if (c->hFlags[0] || it > a.maxit + 2) break;
-      batch = tail;
-    }
+    const int it = pcg_iterate(c, a, amg);
     const int n = c->hFlags[1];
     tot += n;
     c->lastPIts = std::max(1, n);
@@ -746,18 +756,10 @@ void build_slot_lookup(anb_ctx* c) {
 
 void release_amg(anb_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
-  for (auto& g : c->amg.graph) {
-    if (g) cudaGraphExecDestroy(g);
-    g = nullptr;
-  }
-  c->amg.graphKernels = 0;
+  amg_release_graphs(c->amg);
   c->amg.nLevels = 0;
   c->amg.dense = nullptr;
-  for (auto& g : c->amg32.graph) {
-    if (g) cudaGraphExecDestroy(g);
-    g = nullptr;
-  }
-  c->amg32.graphKernels = 0;
+  amg_release_graphs(c->amg32);
   c->amg32.nLevels = 0;
   c->amg32.dense = nullptr;
   c->amgArena.release();
@@ -1052,7 +1054,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     c->amg32.omega = c->amg.omega;
     c->amg32.corr = c->amg.corr;
     c->scal = A.alloc<double>(64);
-    c->flags = A.alloc<int>(32);
+    c->flags = A.alloc<int>(kFlagCount);
     c->stats = A.alloc<double>(16);
     c->forceOut = A.alloc<double>(16);
     c->red.partials = A.alloc<double>((size_t)(c->lc.rowBlocks + 16) * 16);
@@ -1064,7 +1066,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     }
     CK(cudaMemset(c->phi, 0, sizeof(double) * F));
     CK(cudaMemset(c->Pc, 0, sizeof(double) * C));
-    CK(cudaMallocHost(&c->hFlags, sizeof(int) * 32));
+    CK(cudaMallocHost(&c->hFlags, sizeof(int) * kFlagCount));
     CK(cudaMallocHost(&c->hScal, sizeof(double) * 64));
     CK(cudaMallocHost(&c->hStage, sizeof(double) * 3 * C));
     CK(cudaDeviceSynchronize());
@@ -1088,10 +1090,9 @@ void anb_destroy(anb_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->prm.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (auto g : c->amg.graph)
-    if (g) cudaGraphExecDestroy(g);
-  for (auto g : c->amg32.graph)
-    if (g) cudaGraphExecDestroy(g);
+  amg_release_graphs(c->amg);
+  amg_release_graphs(c->amg32);
+  amg_release_graphs(c->amgMom);
   for (auto g : c->momGraph)
     if (g) cudaGraphExecDestroy(g);
   adjoint_release(c);

@@ -274,7 +274,7 @@ struct PcgArgsT {
   int mode;           // 0: PCG iteration; 1: plain preconditioner application z = M^-1 r (no update of
                       // x or r, no r.z reduction; fl[0] is the caller's done flag)
   double* sc;         // rz, alpha, beta, eps, rr, pq
-  int* fl;            // done, iters, converged, first
+  int* fl;            // done, iters, converged, first, loop-graph trips (pcg_capture_loop)
   double atol, rtol;
   int maxit;
   Reducer red;
@@ -320,6 +320,10 @@ struct AmgDevT {
   // writes the other one, with the search direction p0 (v = 0) or p1 (v = 1)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int graphKernels = 0;
+  // the PCG iterations of a whole solve as one graph (see pcg_capture_loop), valid for the
+  // arguments it was captured with
+  cudaGraphExec_t loop = nullptr;
+  PcgArgsT<T> loopArgs{};
   // Coarse tail: the CSR levels with at most tailRows rows and the dense level run as one
   // thread-block-cluster kernel of tailCluster CTAs (0: one launch per level and sweep).
   int tailRows = 0;
@@ -350,8 +354,19 @@ void amg_apply(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg,
 template <class T>
 void bicg_iteration_precond(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*apply)(void* ctx, int c, int which),
                             void* ctx);
+// Captures the two V-cycle variants for the PCG arguments a, then the solve loop
+// (pcg_capture_loop); a loop that cannot be built is left out (the host loop runs instead).
 template <class T>
 cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg);
+// After pcg_init and pcg_precondition: runs the solve's iterations as one launch of the loop graph
+// and returns true, or returns false (nothing launched) when there is no loop graph for a.  The
+// iterations run in pairs; fl[4] counts the graph's condition evaluations (2 (fl[4] - 1)
+// iterations were enqueued on the device).
+template <class T>
+bool pcg_loop_launch(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>& amg);
+// Destroys the captured V-cycles and the loop graph (the stream must be idle).
+template <class T>
+void amg_release_graphs(AmgDevT<T>& amg);
 // Sets the coarse tail (levels of at most tailRows rows on one cluster; 0 = off) and picks its
 // cluster size for this device.  Call before amg_capture_graph.
 template <class T>

@@ -362,6 +362,7 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(PcgArgsT<T> a) {
     a.fl[1] = 0;
     a.fl[2] = a.fl[0];
     a.fl[3] = 1;
+    a.fl[4] = 0;
   }
 }
 
@@ -454,6 +455,14 @@ __global__ void __launch_bounds__(kBlock) k_pcg_xr(PcgArgsT<T> a, const T* p) {
     acc[0] += rr * rr;
   }
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) pcg_converged(a, acc[0]);
+}
+
+// Condition of the PCG loop graph (one thread): go on while the solve is not done, for at most
+// maxTrips evaluations (fl[4], zeroed by k_pcg_init, counts them).
+__global__ void k_pcg_loop_cond(cudaGraphConditionalHandle h, int* fl, int maxTrips) {
+  const int t = fl[4] + 1;
+  fl[4] = t;
+  cudaGraphSetConditional(h, (fl[0] == 0 && t < maxTrips) ? 1u : 0u);
 }
 
 // ---------------------------------------------------------------- AMG V-cycle
@@ -1196,12 +1205,11 @@ void pcg_precondition(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T
 // callers keep x, r, r2, p0, p1, q and z at fixed addresses), so the graphs are captured once and
 // replayed for every preconditioner application.
 template <class T>
+static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg);
+
+template <class T>
 cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
-  for (int v = 0; v < 2; ++v)
-    if (amg.graph[v]) {
-      cudaGraphExecDestroy(amg.graph[v]);
-      amg.graph[v] = nullptr;
-    }
+  amg_release_graphs(amg);
   LaunchCfg quiet = lc;
   quiet.prof = nullptr;
   for (int v = 0; v < 2; ++v) {
@@ -1218,21 +1226,114 @@ cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return e;
   }
+  // without the loop graph the host loop runs (ANB_NO_PCG_LOOP=1 leaves it out, for measurements)
+  const char* noLoop = std::getenv("ANB_NO_PCG_LOOP");
+  if (a.mode == 0 && !(noLoop && noLoop[0] == '1')) pcg_capture_loop(lc, a, amg);
+  return cudaSuccess;
+}
+
+// p = z + beta p_old, q = A p of iteration `it` (p0/p1 alternate)
+template <class T>
+static void launch_pq(const LaunchCfg& lc, const PcgArgsT<T>& a, int it) {
+  const T* pOld = (it & 1) ? a.p1 : a.p0;
+  T* pNew = (it & 1) ? a.p0 : a.p1;
+  // algorithmic bytes: 12 B per off-diagonal (value + column) and 40 B per row in FP64; values
+  // and vectors halve in FP32
+  const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
+  ProfScope ps(lc, kKfPcgSpmv, by);
+  with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, W.value>, a, pOld, pNew); });
+}
+
+// The PCG iterations of a solve as one graph: a condition kernel, then a while node whose body
+// is two AMG-PCG iterations (even: p0 -> p1 with V-cycle variant 1; odd: p1 -> p0 with variant 0)
+// and the condition kernel again.  The condition stays set while the solve is not done, for at
+// most maxit / 2 + 3 evaluations; iterations after convergence return at once, as in the host
+// loop.  The kernels are those of pcg_iteration with the same arguments, so the iterates are the
+// same bit for bit.
+template <class T>
+static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
+  if (amg.loop) {
+    cudaGraphExecDestroy(amg.loop);
+    amg.loop = nullptr;
+  }
+  LaunchCfg quiet = lc;
+  quiet.prof = nullptr;
+  const int maxTrips = a.maxit / 2 + 3;
+  const long long before = g_launches.load();
+  cudaGraph_t g = nullptr, body = nullptr;
+  cudaGraphConditionalHandle h{};
+  cudaGraphNode_t pre = nullptr, loop = nullptr;
+  size_t nPre = 1;
+  cudaGraphNodeParams np{};
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(lc.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    k_pcg_loop_cond<<<1, 1, 0, lc.stream>>>(h, a.fl, maxTrips);
+    e = cudaStreamEndCapture(lc.stream, &g);
+  }
+  if (e == cudaSuccess) e = cudaGraphGetNodes(g, &pre, &nPre);
+  if (e == cudaSuccess && nPre != 1) e = cudaErrorInvalidValue;
+  if (e == cudaSuccess) {
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    e = cudaGraphAddNode(&loop, g, &pre, 1, &np);
+  }
+  if (e == cudaSuccess) {
+    body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(lc.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  }
+  if (e == cudaSuccess) {
+    for (int it = 0; it < 2; ++it) {
+      launch_pq(quiet, a, it);
+      vcycle(quiet, a, &amg, (it + 1) & 1);
+    }
+    k_pcg_loop_cond<<<1, 1, 0, lc.stream>>>(h, a.fl, maxTrips);
+    e = cudaStreamEndCapture(lc.stream, &body);
+  }
+  g_launches = before;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&amg.loop, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    amg.loop = nullptr;
+    cudaGetLastError();
+    return e;
+  }
+  amg.loopArgs = a;
   return cudaSuccess;
 }
 
 template <class T>
+static bool same_pcg_buffers(const PcgArgsT<T>& x, const PcgArgsT<T>& y) {
+  return x.A.val == y.A.val && x.A.diag == y.A.diag && x.A.col == y.A.col && x.x == y.x && x.r == y.r &&
+         x.r2 == y.r2 && x.z == y.z && x.p0 == y.p0 && x.p1 == y.p1 && x.q == y.q && x.sc == y.sc &&
+         x.fl == y.fl && x.maxit == y.maxit && x.mode == y.mode && x.red.partials == y.red.partials;
+}
+
+template <class T>
+bool pcg_loop_launch(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>& amg) {
+  if (!amg.loop || !same_pcg_buffers(a, amg.loopArgs)) return false;
+  return cudaGraphLaunch(amg.loop, lc.stream) == cudaSuccess;
+}
+
+template <class T>
+void amg_release_graphs(AmgDevT<T>& amg) {
+  for (auto& g : amg.graph) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  if (amg.loop) cudaGraphExecDestroy(amg.loop);
+  amg.loop = nullptr;
+  amg.graphKernels = 0;
+}
+
+template <class T>
 void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgDevT<T>* amg) {
-  const T* pOld = (it & 1) ? a.p1 : a.p0;
   T* pNew = (it & 1) ? a.p0 : a.p1;
   const bool useAmg = amg && amg->nLevels >= 2;
-  {
-    // algorithmic bytes: 12 B per off-diagonal (value + column) and 40 B per row in FP64;
-    // values and vectors halve in FP32
-    const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
-    ProfScope ps(lc, kKfPcgSpmv, by);
-    with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, W.value>, a, pOld, pNew); });
-  }
+  launch_pq(lc, a, it);
   if (useAmg) {
     // the V-cycle's level-0 sweep applies x += alpha pNew, r -= alpha q: variant (it + 1) & 1 reads
     // the residual this iteration starts from and uses pNew (p1 on even iterations)
@@ -1316,6 +1417,8 @@ void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, floa
   template void pcg_precondition<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*);  \
   template void amg_refresh<T>(const LaunchCfg&, AmgDevT<T>&);                                \
   template cudaError_t amg_capture_graph<T>(const LaunchCfg&, const PcgArgsT<T>&, AmgDevT<T>&);           \
+  template bool pcg_loop_launch<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>&);  \
+  template void amg_release_graphs<T>(AmgDevT<T>&);                                           \
   template void amg_configure_tail<T>(AmgDevT<T>&, int, cudaStream_t);                          \
   template void amg_apply<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*, cudaGraphExec_t*); \
   template void bicg_iteration_precond<T>(const LaunchCfg&, const BicgArgsT<T>&, void (*)(void*, int, int), void*);
