@@ -120,6 +120,39 @@ void mom_apply(void* ctx, int q, int which) {
   amg_apply(c->lc, c->momArgs[2 * q + which], &c->amgMom, &c->momGraph[2 * q + which]);
 }
 
+// The BiCGSTAB iterations after bicg_init until every component is done: one launch of the loop
+// graph when it applies (no preconditioner callback, no BiCGSTAB kernel family being timed), else
+// batches of iterations (most of the previous solve's count, then two) with a poll after each.
+// Iterations after convergence return at once either way.  Returns the iterations enqueued;
+// hFlags holds the component flags afterwards.
+template <class T>
+int bicg_iterate(anb_ctx* c, const BicgArgsT<T>& a, BicgLoopT<T>& loop) {
+  const int fam = c->prof.family;
+  const bool timed = fam == kKfBicgSpmv || fam == kKfBicgVector;
+  if (!timed && bicg_loop_launch(c->lc, a, loop)) {
+    poll(c, a.fl, 13);
+    const int trips = c->hFlags[12];
+    const int enq = 2 * std::max(trips - 1, 0);
+    g_launches += trips + 5LL * enq;
+    return enq;
+  }
+  int done = 0;
+  int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
+  while (true) {
+    for (int k = 0; k < batch; ++k) {
+      if (a.precond) bicg_iteration_precond(c->lc, a, mom_apply, c);
+      else bicg_iteration(c->lc, a);
+    }
+    done += batch;
+    poll(c, a.fl, 12);
+    bool all = true;
+    for (int q = 0; q < a.nc; ++q) all = all && c->hFlags[4 * q];
+    if (all || done > a.maxit + 2) break;
+    batch = 2;
+  }
+  return done;
+}
+
 void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
   ProfScope whole(c->lc, kKfMomentumSolve, 0.0, 0);
   if (c->mixed) return solve_momentum_mixed(c, active, its, conv);
@@ -144,20 +177,7 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
       const int one[4] = {1, 0, 0, 1};
       CK(cudaMemcpyAsync(a.fl + 4 * q, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
     }
-  int done = 0;
-  int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
-  while (true) {
-    for (int k = 0; k < batch; ++k) {
-      if (a.precond) bicg_iteration_precond(c->lc, a, mom_apply, c);
-      else bicg_iteration(c->lc, a);
-    }
-    done += batch;
-    poll(c, a.fl, 12);
-    bool all = true;
-    for (int q = 0; q < 3; ++q) all = all && c->hFlags[4 * q];
-    if (all || done > a.maxit + 2) break;
-    batch = 2;
-  }
+  const int done = bicg_iterate(c, a, c->momLoop);
   int mx = 0;
   for (int q = 0; q < 3; ++q) {
     its[q] = active[q] ? c->hFlags[4 * q + 2] : 0;
@@ -463,17 +483,7 @@ void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3
     a.atol = 0.5 * target;
     bicg_init(c->lc, a);
     CK(cudaMemcpyAsync(a.fl, innerFlags, sizeof(innerFlags), cudaMemcpyHostToDevice, c->stream));
-    int done = 0;
-    int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
-    while (true) {
-      for (int k = 0; k < batch; ++k) bicg_iteration(c->lc, a);
-      done += batch;
-      poll(c, a.fl, 12);
-      bool fin = true;
-      for (int q = 0; q < 3; ++q) fin = fin && c->hFlags[4 * q];
-      if (fin || done > a.maxit + 2) break;
-      batch = 2;
-    }
+    bicg_iterate(c, a, c->momLoop32);
     int mx = 0;
     for (int q = 0; q < 3; ++q) {
       tot[q] += c->hFlags[4 * q + 2];
@@ -1093,6 +1103,8 @@ void anb_destroy(anb_ctx* c) {
   amg_release_graphs(c->amg);
   amg_release_graphs(c->amg32);
   amg_release_graphs(c->amgMom);
+  bicg_loop_release(c->momLoop);
+  bicg_loop_release(c->momLoop32);
   for (auto g : c->momGraph)
     if (g) cudaGraphExecDestroy(g);
   adjoint_release(c);

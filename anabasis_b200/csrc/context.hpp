@@ -145,6 +145,9 @@ struct anb_ctx {
   double *mwdinv = nullptr, *momScratch = nullptr, *momSc = nullptr;
   PcgArgs momArgs[6] = {};
   cudaGraphExec_t momGraph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // momentum BiCGSTAB iterations as one graph launch (FP64, and the FP32 inner solves)
+  BicgLoopT<double> momLoop;
+  BicgLoopT<float> momLoop32;
 };
 
 namespace anb {

@@ -248,7 +248,7 @@ struct BicgArgsT {
   T* x;
   T *r, *rh, *p, *v, *s, *t, *ph, *sh;
   double* sc;         // per component 8 scalars: rho, rhoN, alpha, omega, eps, rn, tsum, ssum
-  int* fl;            // per component 4 ints: done, half, iters, converged
+  int* fl;            // per component 4 ints: done, half, iters, converged; fl[12]: loop-graph trips
   double atol, rtol;
   int maxit;
   Reducer red;
@@ -260,6 +260,22 @@ template <class T>
 void bicg_init(const LaunchCfg& lc, const BicgArgsT<T>& a);
 template <class T>
 void bicg_iteration(const LaunchCfg& lc, const BicgArgsT<T>& a);
+
+// The BiCGSTAB iterations of a solve as one graph launch, for the arguments it was captured with.
+template <class T>
+struct BicgLoopT {
+  cudaGraphExec_t exec = nullptr;
+  BicgArgsT<T> args{};
+  bool failed = false;  // capture failed once: the host loop runs
+};
+// After bicg_init: runs the (Jacobi-preconditioned) iterations as one launch of the loop graph,
+// captured into `loop` on first use or when a's buffers changed, and returns true; returns false
+// (nothing launched) with a preconditioner callback, when the graph cannot be built, or under
+// ANB_NO_LOOP_GRAPH=1.  Iterations run in pairs; fl[12] counts the condition evaluations.
+template <class T>
+bool bicg_loop_launch(const LaunchCfg& lc, const BicgArgsT<T>& a, BicgLoopT<T>& loop);
+template <class T>
+void bicg_loop_release(BicgLoopT<T>& loop);
 
 template <class T>
 struct PcgArgsT {

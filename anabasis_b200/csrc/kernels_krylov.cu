@@ -129,6 +129,14 @@ __device__ __forceinline__ bool all_done(const int* fl, int nc) {
   return true;
 }
 
+// Condition of the BiCGSTAB loop graph (one thread): go on while a component is not done, for at
+// most maxTrips evaluations (fl[12], zeroed by k_bicg_init, counts them).
+__global__ void k_bicg_loop_cond(cudaGraphConditionalHandle h, int* fl, int nc, int maxTrips) {
+  const int t = fl[12] + 1;
+  fl[12] = t;
+  cudaGraphSetConditional(h, (!all_done(fl, nc) && t < maxTrips) ? 1u : 0u);
+}
+
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgsT<T> a) {
   __shared__ double sm[6 * 32];
@@ -163,6 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgsT<T> a) {
       f[2] = 0;
       f[3] = f[0];
     }
+    a.fl[12] = 0;
   }
 }
 
@@ -1207,6 +1216,12 @@ void pcg_precondition(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T
 template <class T>
 static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg);
 
+// ANB_NO_LOOP_GRAPH=1 keeps the solver loops on the host (for measurements)
+static bool loop_graphs_off() {
+  const char* s = std::getenv("ANB_NO_LOOP_GRAPH");
+  return s && s[0] == '1';
+}
+
 template <class T>
 cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
   amg_release_graphs(amg);
@@ -1226,9 +1241,7 @@ cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return e;
   }
-  // without the loop graph the host loop runs (ANB_NO_PCG_LOOP=1 leaves it out, for measurements)
-  const char* noLoop = std::getenv("ANB_NO_PCG_LOOP");
-  if (a.mode == 0 && !(noLoop && noLoop[0] == '1')) pcg_capture_loop(lc, a, amg);
+  if (a.mode == 0 && !loop_graphs_off()) pcg_capture_loop(lc, a, amg);  // else the host loop runs
   return cudaSuccess;
 }
 
@@ -1244,33 +1257,24 @@ static void launch_pq(const LaunchCfg& lc, const PcgArgsT<T>& a, int it) {
   with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, W.value>, a, pOld, pNew); });
 }
 
-// The PCG iterations of a solve as one graph: a condition kernel, then a while node whose body
-// is two AMG-PCG iterations (even: p0 -> p1 with V-cycle variant 1; odd: p1 -> p0 with variant 0)
-// and the condition kernel again.  The condition stays set while the solve is not done, for at
-// most maxit / 2 + 3 evaluations; iterations after convergence return at once, as in the host
-// loop.  The kernels are those of pcg_iteration with the same arguments, so the iterates are the
-// same bit for bit.
-template <class T>
-static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
-  if (amg.loop) {
-    cudaGraphExecDestroy(amg.loop);
-    amg.loop = nullptr;
-  }
-  LaunchCfg quiet = lc;
-  quiet.prof = nullptr;
-  const int maxTrips = a.maxit / 2 + 3;
+// A solver loop as one graph: cond(h) (a one-thread kernel that sets the condition h), then a
+// while node whose body is body() followed by cond(h) again.  Launches recorded by body() are not
+// counted in g_launches.  On failure *out is null and the error state is cleared.
+template <class Body, class Cond>
+static cudaError_t capture_while(cudaStream_t s, Body&& body, Cond&& cond, cudaGraphExec_t* out) {
+  *out = nullptr;
   const long long before = g_launches.load();
-  cudaGraph_t g = nullptr, body = nullptr;
+  cudaGraph_t g = nullptr, bodyGraph = nullptr;
   cudaGraphConditionalHandle h{};
   cudaGraphNode_t pre = nullptr, loop = nullptr;
   size_t nPre = 1;
   cudaGraphNodeParams np{};
   cudaError_t e = cudaGraphCreate(&g, 0);
   if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
-  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(lc.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    k_pcg_loop_cond<<<1, 1, 0, lc.stream>>>(h, a.fl, maxTrips);
-    e = cudaStreamEndCapture(lc.stream, &g);
+    cond(h);
+    e = cudaStreamEndCapture(s, &g);
   }
   if (e == cudaSuccess) e = cudaGraphGetNodes(g, &pre, &nPre);
   if (e == cudaSuccess && nPre != 1) e = cudaErrorInvalidValue;
@@ -1282,27 +1286,48 @@ static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, A
     e = cudaGraphAddNode(&loop, g, &pre, 1, &np);
   }
   if (e == cudaSuccess) {
-    body = np.conditional.phGraph_out[0];
-    e = cudaStreamBeginCaptureToGraph(lc.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    bodyGraph = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(s, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   }
   if (e == cudaSuccess) {
-    for (int it = 0; it < 2; ++it) {
-      launch_pq(quiet, a, it);
-      vcycle(quiet, a, &amg, (it + 1) & 1);
-    }
-    k_pcg_loop_cond<<<1, 1, 0, lc.stream>>>(h, a.fl, maxTrips);
-    e = cudaStreamEndCapture(lc.stream, &body);
+    body();
+    cond(h);
+    e = cudaStreamEndCapture(s, &bodyGraph);
   }
   g_launches = before;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&amg.loop, g, 0);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
   if (g) cudaGraphDestroy(g);
   if (e != cudaSuccess) {
-    amg.loop = nullptr;
+    *out = nullptr;
     cudaGetLastError();
-    return e;
   }
-  amg.loopArgs = a;
-  return cudaSuccess;
+  return e;
+}
+
+// The PCG iterations of a solve as one graph (capture_while): the body is two AMG-PCG iterations
+// (even: p0 -> p1 with V-cycle variant 1; odd: p1 -> p0 with variant 0).  The condition stays set
+// while the solve is not done, for at most maxit / 2 + 3 evaluations; iterations after
+// convergence return at once, as in the host loop.  The kernels are those of pcg_iteration with
+// the same arguments, so the iterates are the same bit for bit.
+template <class T>
+static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT<T>& amg) {
+  if (amg.loop) cudaGraphExecDestroy(amg.loop);
+  amg.loop = nullptr;
+  LaunchCfg quiet = lc;
+  quiet.prof = nullptr;
+  const int maxTrips = a.maxit / 2 + 3;
+  const cudaError_t e = capture_while(
+      lc.stream,
+      [&] {
+        for (int it = 0; it < 2; ++it) {
+          launch_pq(quiet, a, it);
+          vcycle(quiet, a, &amg, (it + 1) & 1);
+        }
+      },
+      [&](cudaGraphConditionalHandle h) { k_pcg_loop_cond<<<1, 1, 0, lc.stream>>>(h, a.fl, maxTrips); },
+      &amg.loop);
+  if (e == cudaSuccess) amg.loopArgs = a;
+  return e;
 }
 
 template <class T>
@@ -1327,6 +1352,47 @@ void amg_release_graphs(AmgDevT<T>& amg) {
   if (amg.loop) cudaGraphExecDestroy(amg.loop);
   amg.loop = nullptr;
   amg.graphKernels = 0;
+}
+
+template <class T>
+static bool same_bicg_buffers(const BicgArgsT<T>& x, const BicgArgsT<T>& y) {
+  return x.A.val == y.A.val && x.A.diag == y.A.diag && x.A.col == y.A.col && x.nc == y.nc && x.x == y.x &&
+         x.r == y.r && x.rh == y.rh && x.p == y.p && x.v == y.v && x.s == y.s && x.t == y.t && x.ph == y.ph &&
+         x.sh == y.sh && x.sc == y.sc && x.fl == y.fl && x.maxit == y.maxit && x.precond == y.precond &&
+         x.red.partials == y.red.partials;
+}
+
+// The BiCGSTAB iterations of a solve as one graph (capture_while): two Jacobi-preconditioned
+// iterations per trip, the condition set while a component is not done (at most maxit / 2 + 3
+// evaluations); the kernels of bicg_iteration with the same arguments.
+template <class T>
+bool bicg_loop_launch(const LaunchCfg& lc, const BicgArgsT<T>& a, BicgLoopT<T>& loop) {
+  if (a.precond || loop.failed || loop_graphs_off()) return false;
+  if (loop.exec && !same_bicg_buffers(a, loop.args)) bicg_loop_release(loop);
+  if (!loop.exec) {
+    LaunchCfg quiet = lc;
+    quiet.prof = nullptr;
+    const int maxTrips = a.maxit / 2 + 3;
+    const cudaError_t e = capture_while(
+        lc.stream,
+        [&] {
+          for (int k = 0; k < 2; ++k) bicg_step(quiet, a, nullptr, nullptr);
+        },
+        [&](cudaGraphConditionalHandle h) { k_bicg_loop_cond<<<1, 1, 0, lc.stream>>>(h, a.fl, a.nc, maxTrips); },
+        &loop.exec);
+    if (e != cudaSuccess) {
+      loop.failed = true;
+      return false;
+    }
+    loop.args = a;
+  }
+  return cudaGraphLaunch(loop.exec, lc.stream) == cudaSuccess;
+}
+
+template <class T>
+void bicg_loop_release(BicgLoopT<T>& loop) {
+  if (loop.exec) cudaGraphExecDestroy(loop.exec);
+  loop.exec = nullptr;
 }
 
 template <class T>
@@ -1419,6 +1485,8 @@ void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, floa
   template cudaError_t amg_capture_graph<T>(const LaunchCfg&, const PcgArgsT<T>&, AmgDevT<T>&);           \
   template bool pcg_loop_launch<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>&);  \
   template void amg_release_graphs<T>(AmgDevT<T>&);                                           \
+  template bool bicg_loop_launch<T>(const LaunchCfg&, const BicgArgsT<T>&, BicgLoopT<T>&);     \
+  template void bicg_loop_release<T>(BicgLoopT<T>&);                                          \
   template void amg_configure_tail<T>(AmgDevT<T>&, int, cudaStream_t);                          \
   template void amg_apply<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*, cudaGraphExec_t*); \
   template void bicg_iteration_precond<T>(const LaunchCfg&, const BicgArgsT<T>&, void (*)(void*, int, int), void*);

@@ -1,8 +1,9 @@
-"""The pressure solve's iterations as one graph launch (a while node over pairs of AMG-PCG iterations).
+"""Solver loops as one graph launch: a while node over pairs of AMG-PCG iterations (pressure) or
+of Jacobi-BiCGSTAB iterations (momentum), its condition set on the device.
 
-The loop graph replays the same kernels with the same arguments as the host-driven loop
-(main.cu:3450-3520 is the reference's pressure solve, HYPRE PCG), so the fields and the iteration
-counts of a few SIMPLE steps must equal those of a context built with ANB_NO_PCG_LOOP=1 bit for bit,
+The loop graphs replay the same kernels with the same arguments as the host-driven loops (the
+reference's HYPRE PCG and BiCGSTAB solves, apps/generic_simple_v1/src/main.cu:2584-2641 and 2570), so the fields and the
+iteration counts of a few SIMPLE steps must equal those of a run with ANB_NO_LOOP_GRAPH=1 bit for bit,
 in FP64 and in the mixed-precision inner solves, also when every solve is done at its start.
 """
 import os
@@ -20,7 +21,7 @@ PRM = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3)
 
 def _run(m, bc, steps, no_loop, **kw):
     if no_loop:
-        os.environ["ANB_NO_PCG_LOOP"] = "1"
+        os.environ["ANB_NO_LOOP_GRAPH"] = "1"
     try:
         s = anb.Solver(m, anb.default_params(**PRM, **kw))
         s.set_bc(bc)
@@ -29,7 +30,7 @@ def _run(m, bc, steps, no_loop, **kw):
         g = s.get_state()
         s.close()
     finally:
-        os.environ.pop("ANB_NO_PCG_LOOP", None)
+        os.environ.pop("ANB_NO_LOOP_GRAPH", None)
     return g, st
 
 
@@ -40,7 +41,8 @@ def test_loop_graph_matches_host_loop(kw):
     g1, st1 = _run(m, bc, 6, False, **kw)
     for k in ("u", "v", "w", "p", "phi"):
         assert np.array_equal(g0[k], g1[k]), k
-    assert [x["its_p_total"] for x in st0] == [x["its_p_total"] for x in st1]
+    for key in ("its_p_total", "its_u", "its_v", "its_w"):
+        assert [x[key] for x in st0] == [x[key] for x in st1], key
 
 
 def test_solve_done_at_init():
