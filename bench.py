@@ -186,7 +186,6 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     lib = anb.lib()
     # warm-up (includes the one-time AMG structure set-up)
     s.iterate(args.warmup)
-    lib.anb_profile_select(s._h, KERNEL_FAMILY)
     if dist:
         dist.barrier()
     launches0 = lib.anb_launch_count()
@@ -196,10 +195,17 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         wall = time.perf_counter() - t0
     launches = lib.anb_launch_count() - launches0
     dev_seconds = float(sum(x["iter_seconds"] for x in st))
+    # The roofline kernel is timed with a CUDA event pair around each of its launches over the K
+    # steps that follow the timed region (same workload, same launches).  Inside the timed region
+    # the events would keep the pressure solves on the host loop (a graph's while body cannot
+    # record events) and add ~0.4 ms per step at this size.
+    lib.anb_profile_select(s._h, KERNEL_FAMILY)
+    s.iterate(args.steps)
     n_l = ct_ll()
     secs = np.zeros(1)
     byts = np.zeros(1)
     lib.anb_profile_read(s._h, n_l, anb._d(secs), anb._d(byts))
+    lib.anb_profile_select(s._h, 0)
     # end-to-end through the public API: host arrays in, one SIMPLE step, host arrays out
     g = s.get_state(with_phi=False)
     e2e_steps = max(1, min(args.steps, 5))
@@ -241,6 +247,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "launches": int(n_l.value), "algorithmic_bytes": byts[0] / max(int(n_l.value), 1),
+                     "window": f"CUDA events around each launch, the {args.steps} steps after the timed region",
                      "traffic": PCG_SPMV_TRAFFIC_BYTES if KERNEL_FAMILY == 7 else None},
         "inner": {"bicgstab_last": [st[-1]["its_u"], st[-1]["its_v"], st[-1]["its_w"]],
                   "pcg_total_last": st[-1]["its_p_total"], "mass_res_last": st[-1]["mass_res"]},
