@@ -108,6 +108,58 @@ void poll(anb_ctx* c, const int* dflags, int count) {
   CK(cudaStreamSynchronize(c->stream));
 }
 
+// Outcome of one linear solve: iterations and convergence per component, or, for a solve that ran
+// as a loop graph with its read-back deferred, the hDefer slot its flags arrive in once the stream
+// has synchronised (resolve_solve).
+struct SolveOut {
+  bool momentum = false;
+  bool resolved = false;
+  int slot = -1;
+  int active[3] = {1, 1, 1};
+  int its[3] = {0, 0, 0};
+  bool conv[3] = {true, true, true};
+  long long kernelsPerIteration = 0;  // loop-graph launch bookkeeping
+};
+
+// Queues the copy of a loop-graph solve's flags into the next hDefer slot; with every slot taken it
+// polls instead (slot -1, flags in hFlags).
+int defer_flags(anb_ctx* c, const int* dflags, int count) {
+  if (c->nDefer >= kDeferSlots) {
+    poll(c, dflags, count);
+    return -1;
+  }
+  const int slot = c->nDefer++;
+  CK(cudaMemcpyAsync(c->hDefer + slot * kDeferInts, dflags, sizeof(int) * count, cudaMemcpyDeviceToHost,
+                     c->stream));
+  return slot;
+}
+
+// Fills a solve's iterations and convergence from its flags (hDefer slot, after the stream has
+// synchronised, or hFlags right after a poll) and books the kernels its loop graph ran: one
+// condition kernel per evaluation, two iterations per body run.
+void resolve_solve(anb_ctx* c, SolveOut& o) {
+  if (o.resolved) return;
+  o.resolved = true;
+  const int* f = o.slot >= 0 ? c->hDefer + o.slot * kDeferInts : c->hFlags;
+  if (o.momentum) {
+    int mx = 0;
+    for (int q = 0; q < 3; ++q) {
+      o.its[q] = o.active[q] ? f[4 * q + 2] : 0;
+      o.conv[q] = o.active[q] ? f[4 * q + 3] != 0 : true;
+      mx = std::max(mx, o.its[q]);
+    }
+    c->lastMomIts = std::max(1, mx);
+  } else {
+    o.its[0] = f[1];
+    o.conv[0] = f[2] != 0;
+    c->lastPIts = std::max(1, o.its[0]);
+  }
+  if (o.kernelsPerIteration > 0) {
+    const int trips = f[o.momentum ? 12 : 4];
+    g_launches += trips + 2LL * std::max(trips - 1, 0) * o.kernelsPerIteration;
+  }
+}
+
 // Momentum: nc-component BiCGSTAB + Jacobi on the shared matrix; comps with active[q]==0 are
 // frozen.  Returns per-component iterations and convergence.
 void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3]);
@@ -123,18 +175,23 @@ void mom_apply(void* ctx, int q, int which) {
 // The BiCGSTAB iterations after bicg_init until every component is done: one launch of the loop
 // graph when it applies (no preconditioner callback, no BiCGSTAB kernel family being timed), else
 // batches of iterations (most of the previous solve's count, then two) with a poll after each.
-// Iterations after convergence return at once either way.  Returns the iterations enqueued;
-// hFlags holds the component flags afterwards.
+// Iterations after convergence return at once either way.  Returns the iterations enqueued by the
+// host loop (0 for the loop graph).  Afterwards the flags are in hFlags, or, for the loop graph
+// with `out` given, on their way to out->slot.
 template <class T>
-int bicg_iterate(anb_ctx* c, const BicgArgsT<T>& a, BicgLoopT<T>& loop) {
+int bicg_iterate(anb_ctx* c, const BicgArgsT<T>& a, BicgLoopT<T>& loop, SolveOut* out) {
   const int fam = c->prof.family;
   const bool timed = fam == kKfBicgSpmv || fam == kKfBicgVector;
   if (!timed && bicg_loop_launch(c->lc, a, loop)) {
+    if (out) {
+      out->kernelsPerIteration = 5;
+      out->slot = defer_flags(c, a.fl, 13);
+      return 0;
+    }
     poll(c, a.fl, 13);
     const int trips = c->hFlags[12];
-    const int enq = 2 * std::max(trips - 1, 0);
-    g_launches += trips + 5LL * enq;
-    return enq;
+    g_launches += trips + 10LL * std::max(trips - 1, 0);
+    return 0;
   }
   int done = 0;
   int batch = std::max(2, std::min(3 * c->lastMomIts / 4, 32));
@@ -153,9 +210,17 @@ int bicg_iterate(anb_ctx* c, const BicgArgsT<T>& a, BicgLoopT<T>& loop) {
   return done;
 }
 
-void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
+// Momentum solve.  With defer (and the loop graph), out is resolved after the step's
+// synchronisation (resolve_solve); otherwise on return.
+void solve_momentum(anb_ctx* c, const int* active, SolveOut* out, bool defer) {
   ProfScope whole(c->lc, kKfMomentumSolve, 0.0, 0);
-  if (c->mixed) return solve_momentum_mixed(c, active, its, conv);
+  out->momentum = true;
+  for (int q = 0; q < 3; ++q) out->active[q] = active[q];
+  if (c->mixed) {
+    solve_momentum_mixed(c, active, out->its, out->conv);
+    out->resolved = true;
+    return;
+  }
   BicgArgs a{};
   a.A = mom_sell(c);
   a.nc = 3;
@@ -177,14 +242,10 @@ void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]) {
       const int one[4] = {1, 0, 0, 1};
       CK(cudaMemcpyAsync(a.fl + 4 * q, one, sizeof(one), cudaMemcpyHostToDevice, c->stream));
     }
-  const int done = bicg_iterate(c, a, c->momLoop);
-  int mx = 0;
-  for (int q = 0; q < 3; ++q) {
-    its[q] = active[q] ? c->hFlags[4 * q + 2] : 0;
-    conv[q] = active[q] ? c->hFlags[4 * q + 3] != 0 : true;
-    mx = std::max(mx, its[q]);
-  }
-  c->lastMomIts = std::max(1, mx);
+  const int done = bicg_iterate(c, a, c->momLoop, defer ? out : nullptr);
+  if (defer && out->slot >= 0) return;
+  resolve_solve(c, *out);
+  const int* its = out->its;
   if (c->prof.family == kKfBicgSpmv) {  // count only the components each launch worked on
     double booked = 2.0 * done * c->ab.bicg_spmv(3), real = 0.0;
     long long realLaunches = 0;
@@ -225,17 +286,23 @@ PcgArgs pcg_args(anb_ctx* c, const double* b, double rtol) {
 // hierarchy's loop graph when it holds one for these arguments (and no PCG or V-cycle kernel family
 // is being timed), else batches of pcg_iteration, most of the expected iterations (previous
 // solve's count) before the first poll, then small batches.  Iterations after convergence return
-// at once either way.  Returns the iterations enqueued; hFlags holds the PCG flags afterwards.
+// at once either way.  Returns the iterations enqueued by the host loop (0 for the loop graph).
+// Afterwards the PCG flags are in hFlags, or, for the loop graph with `out` given, on their way to
+// out->slot.
 template <class T>
-int pcg_iterate(anb_ctx* c, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
+int pcg_iterate(anb_ctx* c, const PcgArgsT<T>& a, const AmgDevT<T>* amg, SolveOut* out = nullptr) {
   const int fam = c->prof.family;
   const bool timed = fam >= kKfPcgSpmv && fam <= kKfPcgUpdate;
   if (amg && !timed && pcg_loop_launch(c->lc, a, *amg)) {
+    if (out) {
+      out->kernelsPerIteration = 1 + amg->graphKernels;
+      out->slot = defer_flags(c, a.fl, 5);
+      return 0;
+    }
     poll(c, a.fl, 5);
     const int trips = c->hFlags[4];
-    const int enq = 2 * std::max(trips - 1, 0);
-    g_launches += trips + (long long)enq * (1 + amg->graphKernels);
-    return enq;
+    g_launches += trips + 2LL * std::max(trips - 1, 0) * (1 + amg->graphKernels);
+    return 0;
   }
   int it = 0;
   int batch = std::max(2, std::min(3 * c->lastPIts / 4, 64));
@@ -249,24 +316,36 @@ int pcg_iterate(anb_ctx* c, const PcgArgsT<T>& a, const AmgDevT<T>* amg) {
   return it;
 }
 
-// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.
-void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+// Pressure: PCG with the AMG (or Jacobi) preconditioner; x holds the initial guess.  With defer
+// (and the loop graph), out is resolved after the step's synchronisation (resolve_solve);
+// otherwise on return.
+void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, SolveOut* out, bool defer) {
   ProfScope whole(c->lc, kKfPressureSolve, 0.0, 0);
-  if (c->mixed) return solve_pressure_mixed(c, b, x, rtol, its, conv);
+  if (c->mixed) {
+    solve_pressure_mixed(c, b, x, rtol, &out->its[0], &out->conv[0]);
+    out->resolved = true;
+    return;
+  }
   PcgArgs a = pcg_args(c, b, rtol);
   const AmgDev* amg = (c->prm.p_use_amg && c->amgBuilt && c->amg.nLevels >= 2) ? &c->amg : nullptr;
   CK(cudaMemcpyAsync(c->pxw, x, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
   pcg_init(c->lc, a);
   pcg_precondition(c->lc, a, amg);
-  const int it = pcg_iterate(c, a, amg);
+  const int it = pcg_iterate(c, a, amg, defer ? out : nullptr);
   CK(cudaMemcpyAsync(x, c->pxw, sizeof(double) * c->C, cudaMemcpyDeviceToDevice, c->stream));
-  *its = c->hFlags[1];
-  *conv = c->hFlags[2] != 0;
-  c->lastPIts = std::max(1, *its);
+  if (defer && out->slot >= 0) return;
+  resolve_solve(c, *out);
   if (c->prof.family == kKfPcgSpmv) {  // launches after convergence returned at once: not counted
-    c->prof.bytes -= (double)(it - *its) * c->ab.pcg_spmv();
-    c->prof.launches -= it - *its;
+    c->prof.bytes -= (double)(it - out->its[0]) * c->ab.pcg_spmv();
+    c->prof.launches -= it - out->its[0];
   }
+}
+
+void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv) {
+  SolveOut o;
+  solve_pressure(c, b, x, rtol, &o, false);
+  *its = o.its[0];
+  *conv = o.conv[0];
 }
 
 PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, double rtol) {
@@ -483,7 +562,7 @@ void solve_momentum_mixed(anb_ctx* c, const int* active, int its[3], bool conv[3
     a.atol = 0.5 * target;
     bicg_init(c->lc, a);
     CK(cudaMemcpyAsync(a.fl, innerFlags, sizeof(innerFlags), cudaMemcpyHostToDevice, c->stream));
-    bicg_iterate(c, a, c->momLoop32);
+    bicg_iterate(c, a, c->momLoop32, nullptr);
     int mx = 0;
     for (int q = 0; q < 3; ++q) {
       tot[q] += c->hFlags[4 * q + 2];
@@ -605,6 +684,10 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   CK(cudaEventCreate(&e1));
   CK(cudaEventRecord(e0, c->stream));
   ++c->outerStep;
+  // solves whose flags are read back after the step's one synchronisation
+  c->nDefer = 0;
+  std::vector<SolveOut> pending;
+  pending.reserve(8);
   // 1. gradients of the old fields (u, v, w with their BC sets, p)
   {
     const double* phi[4] = {c->U, c->U + C, c->U + 2 * C, c->P};
@@ -634,14 +717,17 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
       // keep the iterate for the relative-change test (main.cu:3377-3381)
       if (nVel > 1 && it < nVel)
         CK(cudaMemcpyAsync(c->UsPrev, c->Us, sizeof(double) * 3 * C, cudaMemcpyDeviceToDevice, c->stream));
-      int itq[3];
-      bool cv[3];
-      solve_momentum(c, active, itq, cv);
-      for (int q = 0; q < 3; ++q)
-        if (active[q]) {
-          its[q] = itq[q];
-          anyNC = anyNC || !cv[q];
-        }
+      SolveOut mo;
+      solve_momentum(c, active, &mo, nVel == 1);
+      if (!mo.resolved) {
+        pending.push_back(mo);  // the only momentum pass: its flags arrive with the step's sync
+      } else {
+        for (int q = 0; q < 3; ++q)
+          if (active[q]) {
+            its[q] = mo.its[q];
+            anyNC = anyNC || !mo.conv[q];
+          }
+      }
       if (nVel > 1 && it < nVel) {
         // relchg = sqrt(sum (q_new - q_iter)^2 / (1 + sum q_new^2)) per component, reduced on the device
         launch_relchg3(c->lc, C, c->UsPrev, c->Us, c->red, c->scal + kScalRelchg);
@@ -690,11 +776,9 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
     }
     ++counter;
     const double rtol = counter == total ? 0.0 : p.p_rel_tol;
-    bool cv = true;
     if (perSolve && pc > 1) ensure_amg(c);
-    solve_pressure(c, c->pb, c->Pc, rtol, &pLast, &cv);
-    anyNC = anyNC || !cv;
-    pTot += pLast;
+    pending.emplace_back();
+    solve_pressure(c, c->pb, c->Pc, rtol, &pending.back(), true);
     if (pc == nPS) {
       const double* phi[1] = {c->Pc};
       double* out[1] = {c->Gc};
@@ -708,11 +792,9 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
     launch_pass_rhs(c->lc, C, c->divCorr, c->pb, c->pdx);
     ++counter;
     const double rtol = counter == total ? 0.0 : p.p_rel_tol;
-    bool cv = true;
     if (perSolve) ensure_amg(c);
-    solve_pressure(c, c->pb, c->pdx, rtol, &pLast, &cv);
-    anyNC = anyNC || !cv;
-    pTot += pLast;
+    pending.emplace_back();
+    solve_pressure(c, c->pb, c->pdx, rtol, &pending.back(), true);
     launch_add_scaled(c->lc, C, 1.0, c->pdx, c->Pc);
     const double* phi[1] = {c->Pc};
     double* out[1] = {c->Gc};
@@ -724,6 +806,20 @@ int simple_step(anb_ctx* c, anb_iter_stats* st) {
   CK(cudaMemcpyAsync(c->hScal, c->stats, sizeof(double) * 9, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
+  for (SolveOut& o : pending) {
+    resolve_solve(c, o);
+    if (o.momentum) {
+      for (int q = 0; q < 3; ++q)
+        if (o.active[q]) {
+          its[q] = o.its[q];
+          anyNC = anyNC || !o.conv[q];
+        }
+    } else {
+      pLast = o.its[0];
+      pTot += pLast;
+      anyNC = anyNC || !o.conv[0];
+    }
+  }
   c->prof.flush();
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, e0, e1));
@@ -1079,6 +1175,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     CK(cudaMallocHost(&c->hFlags, sizeof(int) * kFlagCount));
     CK(cudaMallocHost(&c->hScal, sizeof(double) * 64));
     CK(cudaMallocHost(&c->hStage, sizeof(double) * 3 * C));
+    CK(cudaMallocHost(&c->hDefer, sizeof(int) * kDeferSlots * kDeferInts));
     CK(cudaDeviceSynchronize());
     lap(3);
     return ANB_OK;
@@ -1089,7 +1186,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->hFlags) cudaFreeHost(c->hFlags);
     if (c->hScal) cudaFreeHost(c->hScal);
-  if (c->hStage) cudaFreeHost(c->hStage);
+    if (c->hStage) cudaFreeHost(c->hStage);
+    if (c->hDefer) cudaFreeHost(c->hDefer);
     return rc;
   }
   *out = c.release();
@@ -1113,6 +1211,7 @@ void anb_destroy(anb_ctx* c) {
   if (c->hFlags) cudaFreeHost(c->hFlags);
   if (c->hScal) cudaFreeHost(c->hScal);
   if (c->hStage) cudaFreeHost(c->hStage);
+  if (c->hDefer) cudaFreeHost(c->hDefer);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

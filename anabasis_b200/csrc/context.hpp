@@ -106,6 +106,10 @@ struct anb_ctx {
   Reducer red{};
   // pinned host mirrors
   int* hFlags = nullptr;
+  // flags of the solves that ran as loop graphs in the current step, copied here asynchronously
+  // and read after the step's one synchronisation (kDeferSlots slots of kDeferInts ints)
+  int* hDefer = nullptr;
+  int nDefer = 0;
   double* hScal = nullptr;
   double* hStage = nullptr;   // 3 * nCells staging for cell fields
   // state
@@ -157,6 +161,8 @@ constexpr int kScalPcg = 24;    // 8
 constexpr int kFlagBicg = 0;    // 3 * 4
 constexpr int kFlagPcg = 32;    // 8: done, iterations, converged, first, loop-graph trips
 constexpr int kFlagCount = 40;  // ints in anb_ctx::flags (and hFlags)
+constexpr int kDeferSlots = 64;
+constexpr int kDeferInts = 16;
 constexpr int kScalRelchg = 56; // 6: momentum relative-change sums
 
 int fail(anb_ctx* c, const AnbError& e);
