@@ -443,10 +443,6 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, std::vector<AmgLevelHost>& H, DevArena
   amg_configure_tail(A, tailEnv ? std::atoi(tailEnv) : kAmgTailRows, c->stream);
   const char* fdEnv = std::getenv("ANB_AMG_FUSED_DOWN_ROWS");
   A.fusedDownRows = fdEnv ? std::atoi(fdEnv) : kAmgFusedDownRows;
-  if (const char* sl = std::getenv("ANB_AMG_SELL_LANES")) {  // 1, 2, 4 or 8
-    const int g = std::atoi(sl);
-    A.sellLanes = (g == 1 || g == 2 || g == 8) ? g : 4;
-  }
   const char* verbose = std::getenv("ANB_AMG_VERBOSE");
   if (verbose && verbose[0] == '1') {
     std::fprintf(stderr, "AMG levels (rows/stored entries/max width):");

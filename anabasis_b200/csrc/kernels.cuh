@@ -347,9 +347,6 @@ struct AmgDevT {
   // CSR levels of at most this many rows (above the tail) run their down sweep and restriction
   // as one kernel, warp per aggregate (same values; fewer launches, longer chains per warp)
   int fusedDownRows = 0;
-  // lanes per row of the coarse SELL levels whose rows exceed the register classes (1: one thread
-  // per row, the level-0 kernels' generic loop)
-  int sellLanes = 4;
 };
 using AmgLevelDev = AmgLevelDevT<double>;
 using AmgDev = AmgDevT<double>;

@@ -782,75 +782,6 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
   }
 }
 
-// Coarse SELL-32 levels whose rows are longer than the register classes (level 1 of a hex mesh:
-// ~14 entries, slices ~17 slots wide): G lanes per row, lane g takes slots g, g + G, ... of the
-// row and the partial sums meet through shuffles, so a row costs ~W / G dependent load chains
-// instead of W.  A warp covers 32 / G consecutive rows of one slice: each slot step reads G runs
-// of 32 / G consecutive entries.  Padding slots (column = the row, value 0) add zero.  The loop
-// bound is uniform over the warp, so every lane reaches the shuffles.
-template <class T, int G>
-__global__ void __launch_bounds__(kBlock) k_amg_resid_sg(const int* done, AmgLevelDevT<T> f) {
-  if (*done) return;
-  constexpr int RPW = 32 / G;
-  const int lane = threadIdx.x & 31, sub = lane % G;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * RPW; base < f.n; base += nWarps * RPW) {
-    const int i = base + lane / G;
-    double acc = 0.0;
-    if (i < f.n) {
-      const int s = i >> 5;
-      const int b0 = __ldg(&f.sliceOff[s]);
-      const int W = (__ldg(&f.sliceOff[s + 1]) - b0) >> 5;
-      const int b = b0 + (i & 31);
-#pragma unroll 4
-      for (int k = sub; k < W; k += G) {
-        const int e = b + (k << 5);
-        const int j = __ldg(&f.col[e]);
-        acc += ld(&f.val[e]) * (ld(&f.wdinv[j]) * ld(&f.b[j]));
-      }
-    }
-    acc = group_sum<G>(acc);
-    if (i < f.n && sub == 0) {
-      const double di = ld(&f.diag[i]), bi = ld(&f.b[i]);
-      const double xi = ld(&f.wdinv[i]) * bi;
-      f.x[i] = (T)xi;
-      f.x2[i] = (T)(bi - di * xi - acc);
-    }
-  }
-}
-
-// Up sweep of such a level: out = xt + w D^-1 (b - A xt), xt = x + corr e[agg] (G lanes per row).
-template <class T, int G>
-__global__ void __launch_bounds__(kBlock) k_amg_up_sg(const int* done, AmgLevelDevT<T> f, const T* e, double corr,
-                                                      T* out) {
-  if (*done) return;
-  constexpr int RPW = 32 / G;
-  const int lane = threadIdx.x & 31, sub = lane % G;
-  const int nWarps = (gridDim.x * blockDim.x) >> 5;
-  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * RPW; base < f.n; base += nWarps * RPW) {
-    const int i = base + lane / G;
-    double acc = 0.0;
-    if (i < f.n) {
-      const int s = i >> 5;
-      const int b0 = __ldg(&f.sliceOff[s]);
-      const int W = (__ldg(&f.sliceOff[s + 1]) - b0) >> 5;
-      const int b = b0 + (i & 31);
-#pragma unroll 4
-      for (int k = sub; k < W; k += G) {
-        const int ee = b + (k << 5);
-        const int j = __ldg(&f.col[ee]);
-        acc += ld(&f.val[ee]) * (ld(&f.x[j]) + corr * ld(&e[__ldg(&f.agg[j])]));
-      }
-    }
-    acc = group_sum<G>(acc);
-    if (i < f.n && sub == 0) {
-      const double di = ld(&f.diag[i]);
-      const double xi = ld(&f.x[i]) + corr * ld(&e[__ldg(&f.agg[i])]);
-      out[i] = (T)(xi + ld(&f.wdinv[i]) * (ld(&f.b[i]) - di * xi - acc));
-    }
-  }
-}
-
 // Coarsest level on its own: one block.
 template <class T>
 __global__ void k_amg_dense_apply(const int* done, int n, const double* inv, const T* b, T* x) {
@@ -1211,15 +1142,6 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     for (int l = 1; l < t0; ++l) {
       const AmgLevelDevT<T>& f = amg->lv[l];
       if (f.sliceOff) {  // large coarse level in SELL-32: the level-0 kernels, thread per row
-        if (launch_width_class(f.maxW) == 0 && amg->sellLanes > 1) {  // long rows: several lanes per row
-          const int g = amg->sellLanes;
-          const int nb = blocks_for(f.n * g, lc.rowBlocks);
-          if (g == 2) launch_rows(lc, nb, k_amg_resid_sg<T, 2>, a.fl, f);
-          else if (g == 8) launch_rows(lc, nb, k_amg_resid_sg<T, 8>, a.fl, f);
-          else launch_rows(lc, nb, k_amg_resid_sg<T, 4>, a.fl, f);
-          k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
-          continue;
-        }
         const int nb = blocks_for(f.n, lc.rowBlocks);
         with_width(f.maxW, [&](auto W) { launch_rows(lc, nb, k_amg_resid<T, W.value>, a.fl, f, amg->omega); });
         k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
@@ -1245,14 +1167,6 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
       // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
       const T* e = (l + 1 == L - 1) ? amg->lv[l + 1].x : amg->lv[l + 1].x2;
       if (f.sliceOff) {
-        if (launch_width_class(f.maxW) == 0 && amg->sellLanes > 1) {
-          const int g = amg->sellLanes;
-          const int nb = blocks_for(f.n * g, lc.rowBlocks);
-          if (g == 2) launch_rows(lc, nb, k_amg_up_sg<T, 2>, a.fl, f, e, amg->corr, f.x2);
-          else if (g == 8) launch_rows(lc, nb, k_amg_up_sg<T, 8>, a.fl, f, e, amg->corr, f.x2);
-          else launch_rows(lc, nb, k_amg_up_sg<T, 4>, a.fl, f, e, amg->corr, f.x2);
-          continue;
-        }
         const int nb = blocks_for(f.n, lc.rowBlocks);
         with_width(f.maxW, [&](auto W) {
           launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
