@@ -429,6 +429,14 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, std::vector<AmgLevelHost>& H, DevArena
       d.agg = ar.upload(h.agg);
       d.memOff = ar.upload(h.memOff);
       d.mem = ar.upload(h.mem);
+      if (l > 0 && h.sliceOff.empty()) {  // CSR level: the sweeps' shortcut indices
+        std::vector<int> colAgg(h.col.size());
+        for (size_t k = 0; k < h.col.size(); ++k) colAgg[k] = h.agg[h.col[k]];
+        std::vector<int2> memRow(h.mem.size());
+        for (size_t m = 0; m < h.mem.size(); ++m) memRow[m] = make_int2(h.rowOff[h.mem[m]], h.rowOff[h.mem[m] + 1]);
+        d.colAgg = ar.upload(colAgg);
+        d.memRow = ar.upload(memRow);
+      }
       d.gOff = ar.upload(h.gOff);
       d.gIdx = ar.upload(h.gIdx);
       d.nEntNext = H[l + 1].nStore;

@@ -312,6 +312,10 @@ struct AmgLevelDevT {
   const int* agg;
   const int* memOff;
   const int* mem;
+  // CSR levels: agg[col[k]] per stored entry, and the entry range {rowOff[i], rowOff[i + 1]} of
+  // member mem[m] per member slot m; they take one dependent load out of the up and down sweeps
+  const int* colAgg;
+  const int2* memRow;
   const int* gOff;     // Galerkin gather for the next level's storage
   const int* gIdx;
   int nEntNext;        // next level's SELL storage entries

@@ -634,8 +634,9 @@ __device__ __forceinline__ void down_csr_aggs(const AmgLevelDevT<T>& f, T* bNext
       int i = 0;
       if (mm < m1) {
         i = __ldg(&f.mem[mm]);
-        const int k1 = __ldg(&f.rowOff[i + 1]);
-        for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
+        const int2 kr = __ldg(&f.memRow[mm]);
+        const int k1 = kr.y;
+        for (int k = kr.x + sub; k < k1; k += G) {
           const int j = __ldg(&f.col[k]);
           acc += ld(&f.val[k]) * (ld(&f.wdinv[j]) * ldv(&f.b[j]));
         }
@@ -671,7 +672,7 @@ __device__ __forceinline__ void up_csr_rows(const AmgLevelDevT<T>& f, const T* e
       const int k1 = __ldg(&f.rowOff[i + 1]);
       for (int k = __ldg(&f.rowOff[i]) + sub; k < k1; k += G) {
         const int j = __ldg(&f.col[k]);
-        acc += ld(&f.val[k]) * (ldv(&f.x[j]) + corr * ldv(&e[__ldg(&f.agg[j])]));
+        acc += ld(&f.val[k]) * (ldv(&f.x[j]) + corr * ldv(&e[__ldg(&f.colAgg[k])]));
       }
     }
     acc = group_sum<G>(acc);
