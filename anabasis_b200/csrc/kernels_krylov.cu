@@ -188,12 +188,22 @@ __global__ void __launch_bounds__(kBlock) k_bicg_p(BicgArgsT<T> a) {
     beta[c] = (s[1] / s[0]) * (s[2] / s[3]);
     om[c] = s[3];
   }
+  // every load of a row (all components) is issued before its stores, which the compiler must
+  // otherwise assume alias the next component's inputs
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const double dinv = 1.0 / (double)a.A.diag[r];
+    double rv[3], pv[3], vv[3];
     _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
-      const double pn = (double)a.r[i] + beta[c] * ((double)a.p[i] - om[c] * (double)a.v[i]);
+      rv[c] = ld(&a.r[i]);
+      pv[c] = (double)a.p[i];
+      vv[c] = ld(&a.v[i]);
+    }
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
+      if (!act[c]) continue;
+      const size_t i = (size_t)c * n + r;
+      const double pn = rv[c] + beta[c] * (pv[c] - om[c] * vv[c]);
       a.p[i] = (T)pn;
       if (!a.precond) a.ph[i] = (T)(dinv * pn);
     }
@@ -248,10 +258,17 @@ __global__ void __launch_bounds__(kBlock) k_bicg_s(BicgArgsT<T> a) {
   double acc[3] = {0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const double dinv = 1.0 / (double)a.A.diag[r];
+    double rv[3], vv[3];
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {  // loads first, as in k_bicg_p
+      if (!act[c]) continue;
+      const size_t i = (size_t)c * n + r;
+      rv[c] = ld(&a.r[i]);
+      vv[c] = ld(&a.v[i]);
+    }
     _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
-      const double sv = (double)a.r[i] - al[c] * (double)a.v[i];
+      const double sv = rv[c] - al[c] * vv[c];
       a.s[i] = (T)sv;
       if (!a.precond) a.sh[i] = (T)(dinv * sv);
       acc[c] += sv * sv;
@@ -310,17 +327,30 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgsT<T> a) {
   }
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double xv[3], phv[3], shv[3], sv[3], tv[3], rhv[3];
+    _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {  // loads first, as in k_bicg_p
+      if (!act[c]) continue;
+      const size_t i = (size_t)c * n + r;
+      xv[c] = (double)a.x[i];
+      phv[c] = ld(&a.ph[i]);
+      if (!half[c]) {
+        shv[c] = ld(&a.sh[i]);
+        sv[c] = ld(&a.s[i]);
+        tv[c] = ld(&a.t[i]);
+        rhv[c] = ld(&a.rh[i]);
+      }
+    }
     _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       if (!act[c]) continue;
       const size_t i = (size_t)c * n + r;
       if (half[c]) {
-        a.x[i] = (T)((double)a.x[i] + al[c] * (double)a.ph[i]);
+        a.x[i] = (T)(xv[c] + al[c] * phv[c]);
       } else {
-        a.x[i] = (T)((double)a.x[i] + al[c] * (double)a.ph[i] + om[c] * (double)a.sh[i]);
-        const double rr = (double)a.s[i] - om[c] * (double)a.t[i];
+        a.x[i] = (T)(xv[c] + al[c] * phv[c] + om[c] * shv[c]);
+        const double rr = sv[c] - om[c] * tv[c];
         a.r[i] = (T)rr;
         acc[2 * c] += rr * rr;
-        acc[2 * c + 1] += (double)a.rh[i] * rr;
+        acc[2 * c + 1] += rhv[c] * rr;
       }
     }
   }
