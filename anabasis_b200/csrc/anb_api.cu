@@ -273,8 +273,6 @@ PcgArgs pcg_args(anb_ctx* c, const double* b, double rtol) {
   a.x = c->pxw;
   a.r = c->pr; a.z = c->pz; a.p0 = c->pp0; a.p1 = c->pp1; a.q = c->pq;
   a.r2 = c->pr2;
-  a.zp[0] = c->pzp;
-  a.zp[1] = c->pzp + 2 * (size_t)c->C;
   a.sc = c->scal + kScalPcg;
   a.fl = c->flags + kFlagPcg;
   a.atol = c->prm.p_tol;
@@ -357,8 +355,6 @@ PcgArgsT<float> pcg_args32(anb_ctx* c, const float* b, float* x, double atol, do
   a.x = x;
   a.r = c->pr32; a.z = c->pz32; a.p0 = c->pp0_32; a.p1 = c->pp1_32; a.q = c->pq32;
   a.r2 = c->pr2_32;
-  a.zp[0] = c->pzp32;
-  a.zp[1] = c->pzp32 + 2 * (size_t)c->C;
   a.sc = c->scal + kScalPcg;
   a.fl = c->flags + kFlagPcg;
   a.atol = atol;
@@ -1129,7 +1125,6 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       c->pz32 = A.alloc<float>(C);
       c->pp0_32 = A.alloc<float>(C);
       c->pp1_32 = A.alloc<float>(C);
-      c->pzp32 = A.alloc<float>(4 * C);
       c->pq32 = A.alloc<float>(C);
       c->pr2_32 = A.alloc<float>(C);
       CK(cudaMemset(c->mval32, 0, sizeof(float) * c->nEnt));
@@ -1152,7 +1147,6 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
       c->pz = A.alloc<double>(C);
       c->pp0 = A.alloc<double>(C);
       c->pp1 = A.alloc<double>(C);
-      c->pzp = A.alloc<double>(4 * C);
       c->pq = A.alloc<double>(C);
       c->pr2 = A.alloc<double>(C);
       c->pxw = A.alloc<double>(C);

@@ -95,7 +95,6 @@ struct anb_ctx {
   double* UsPrev = nullptr;   // momentum iterates before a re-solve (3*C; only with nVelNonOrthCorr > 0)
   double *bw[8] = {nullptr};  // BiCGSTAB work vectors (3*C each)
   double *pr = nullptr, *pz = nullptr, *pp0 = nullptr, *pp1 = nullptr, *pq = nullptr, *pdx = nullptr;
-  double* pzp = nullptr;  // 4n: the two {z, p} pair arrays of the AMG-preconditioned PCG
   // second PCG residual buffer and the PCG iterate at a fixed address (the captured V-cycles update
   // both in place); solve_pressure copies the caller's x in and out
   double *pr2 = nullptr, *pxw = nullptr;
@@ -130,7 +129,6 @@ struct anb_ctx {
   float* bw32[8] = {nullptr};
   float *r32 = nullptr, *dx32 = nullptr;                     // 3*nCells each
   float *pr32 = nullptr, *pz32 = nullptr, *pp0_32 = nullptr, *pp1_32 = nullptr, *pq32 = nullptr, *pr2_32 = nullptr;
-  float* pzp32 = nullptr;
   AmgDevT<float> amg32;
   double innerRtol = 1e-4;    // relative reduction asked of one FP32 inner solve at most
   // scalar-library solves (allocated on first use)

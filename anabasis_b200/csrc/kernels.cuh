@@ -287,10 +287,6 @@ struct PcgArgsT {
   // down sweep applies r_new = r - alpha q and x += alpha p itself, reading the old residual of
   // the neighbour rows from one buffer while it writes the new one into the other.
   T* r2;
-  // AMG-preconditioned iterations: z and p as {z, p} pairs in two arrays of 2n (null: the separate
-  // z, p0, p1).  Iteration `it` reads zp[it & 1] (z and p_old, one load per row) and writes p_new
-  // and, in the V-cycle, the next z into zp[(it + 1) & 1].
-  T* zp[2];
   int mode;           // 0: PCG iteration; 1: plain preconditioner application z = M^-1 r (no update of
                       // x or r, no r.z reduction; fl[0] is the caller's done flag)
   double* sc;         // rz, alpha, beta, eps, rr, pq

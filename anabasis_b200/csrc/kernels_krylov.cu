@@ -465,66 +465,6 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld,
   }
 }
 
-template <class T>
-struct Pair;
-template <>
-struct Pair<double> {
-  using type = double2;
-};
-template <>
-struct Pair<float> {
-  using type = float2;
-};
-
-// k_pcg_pq on interleaved vectors: zpOld holds {z, p_old} pairs, so a row's two values and each
-// neighbour's come in one 16-byte (FP32: 8-byte) load instead of two; p_new goes to the p halves
-// of the other pair array (zpNew[2 r + 1]).  Same arithmetic as k_pcg_pq.
-template <class T, int WM>
-__global__ void __launch_bounds__(kBlock) k_pcg_pq_il(PcgArgsT<T> a, const T* zpOld, T* zpNew) {
-  using V2 = typename Pair<T>::type;
-  __shared__ double sm[32];
-  if (a.fl[0]) return;
-  const int n = a.A.n;
-  // first iteration: p = z, and the p halves are not used (they may hold anything, NaN included)
-  const bool first = a.fl[3] != 0;
-  const double beta = first ? 0.0 : a.sc[2];
-  const V2* zp = reinterpret_cast<const V2*>(zpOld);
-  auto pval = [first, beta](V2 u) {
-    return first ? (double)u.x : (double)(T)((double)u.x + beta * (double)u.y);
-  };
-  double acc[1] = {0};
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-    const double pr = pval(__ldg(&zp[r]));
-    double q = (double)a.A.diag[r] * pr;
-    if constexpr (WM == 0) {
-      const int s = r >> 5;
-      const int b = __ldg(&a.A.sliceOff[s]) + (r & 31);
-      const int W = (__ldg(&a.A.sliceOff[s + 1]) - __ldg(&a.A.sliceOff[s])) >> 5;
-      for (int k = 0; k < W; ++k) {
-        const int e = b + (k << 5);
-        q += (double)a.A.val[e] * pval(__ldg(&zp[__ldg(&a.A.col[e])]));
-      }
-    } else {
-      int c[WM];
-      double v[WM];
-      sell_regs<WM>(a.A.sliceOff, a.A.col, a.A.val, r, c, v);
-      V2 g[WM];
-#pragma unroll
-      for (int k = 0; k < WM; ++k) g[k] = __ldg(&zp[c[k]]);
-#pragma unroll
-      for (int k = 0; k < WM; ++k) q += v[k] * pval(g[k]);
-    }
-    zpNew[2 * r + 1] = (T)pr;
-    a.q[r] = (T)q;
-    acc[0] += pr * q;
-  }
-  if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    a.sc[5] = acc[0];
-    a.sc[1] = acc[0] != 0.0 ? a.sc[0] / acc[0] : 0.0;
-    a.fl[3] = 0;
-  }
-}
-
 // Iteration count and convergence test on |r|^2 = rr (last block, thread 0).
 template <class T>
 __device__ __forceinline__ void pcg_converged(const PcgArgsT<T>& a, double rr) {
@@ -604,11 +544,10 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid(const int* done, AmgLevelD
 // r_new come from their old residual and q, rounded to T as their own rows store them, so the
 // values are those of a separate update kernel followed by k_amg_resid.  The old residual is read
 // from rIn and the new one written to rOut (other rows still read rIn).  Right after pcg_init
-// (flag "first") there is no update: r_new = r.  p[i * ps]: the search direction (ps = 2 when it
-// is interleaved with z).
+// (flag "first") there is no update: r_new = r.
 template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_amg_resid0(PcgArgsT<T> a, AmgLevelDevT<T> f, const T* rIn, T* rOut,
-                                                       const T* p, int ps) {
+                                                       const T* p) {
   __shared__ double sm[32];
   if (a.fl[0]) return;
   const bool upd = a.mode == 0 && a.fl[3] == 0;
@@ -620,7 +559,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_resid0(PcgArgsT<T> a, AmgLevelDe
       const double rr = __fma_rn(-al, ld(&a.q[i]), ld(&rIn[i]));
       acc[0] += rr * rr;
       ri = (double)(T)rr;
-      a.x[i] = (T)__fma_rn(al, (double)p[(size_t)i * ps], (double)a.x[i]);
+      a.x[i] = (T)__fma_rn(al, (double)p[i], (double)a.x[i]);
     } else {
       ri = ld(&rIn[i]);
     }
@@ -828,11 +767,11 @@ __global__ void __launch_bounds__(kBlock) k_amg_restrict(const int* done, AmgLev
 }
 
 // Up: prolongate the coarse correction and post-smooth (one weighted-Jacobi sweep) in one pass:
-// xt_j = x_j + corr * e[agg(j)] on the fly, out[i * os] = xt_i + w D^-1 (b_i - (A xt)_i).
-// On level 0 it also forms r.z for the PCG recurrence (os = 2 when z is interleaved with p).
+// xt_j = x_j + corr * e[agg(j)] on the fly, out_i = xt_i + w D^-1 (b_i - (A xt)_i).
+// On level 0 it also forms r.z for the PCG recurrence.
 template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevelDevT<T> f, const T* e, double omega,
-                                                   double corr, T* out, int os, int finest, PcgArgsT<T> a) {
+                                                   double corr, T* out, int finest, PcgArgsT<T> a) {
   __shared__ double sm[32];
   if (*doneFlag) return;
   double acc[1] = {0};
@@ -863,7 +802,7 @@ __global__ void __launch_bounds__(kBlock) k_amg_up(const int* doneFlag, AmgLevel
     }
     const double bi = (double)f.b[i];
     const T xn = (T)(xi + ld(&f.wdinv[i]) * (bi - ax));
-    out[(size_t)i * os] = xn;
+    out[i] = xn;
     if (finest) acc[0] += bi * (double)xn;
   }
   if (!finest || a.mode != 0) return;
@@ -1209,24 +1148,20 @@ void amg_configure_tail(AmgDevT<T>& amg, int tailRows, cudaStream_t s) {
 
 // One V-cycle z = M^-1 r_new, fused at level 0 with the PCG update r_new = r - alpha q,
 // x += alpha p (see k_amg_resid0): variant v reads the residual buffer v (0: a.r, 1: a.r2), writes
-// the other and updates x with p_v.  With interleaved pairs (a.zp) p_v is the p half of zp[v] and
-// z goes to the z half of zp[v] (the pair the next iteration's k_pcg_pq_il reads); else p0/p1 and z.
+// the other and updates x with p_v.
 template <class T>
 static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* amg, int v) {
   const int L = amg->nLevels;
   const T* rIn = v ? a.r2 : a.r;
   T* rOut = v ? a.r : a.r2;
-  const bool il = a.zp[0] != nullptr;
-  const T* p = il ? a.zp[v] + 1 : (v ? a.p1 : a.p0);
-  T* z = il ? a.zp[v] : a.z;
-  const int stride = il ? 2 : 1;
+  const T* p = v ? a.p1 : a.p0;
   AmgLevelDevT<T> f0 = amg->lv[0];
   f0.b = rOut;  // level 0 right-hand side is the new PCG residual
   {
     const AmgLevelDevT<T>& f = f0;
     ProfScope ps(lc, kKfAmgResid0, 0.0, 2);
     const int nb = blocks_for(f.n, lc.rowBlocks);
-    with_width(f.maxW, [&](auto W) { launch_rows(lc, nb, k_amg_resid0<T, W.value>, a, f, rIn, rOut, p, stride); });
+    with_width(f.maxW, [&](auto W) { launch_rows(lc, nb, k_amg_resid0<T, W.value>, a, f, rIn, rOut, p); });
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
@@ -1265,7 +1200,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
       if (f.sliceOff) {
         const int nb = blocks_for(f.n, lc.rowBlocks);
         with_width(f.maxW, [&](auto W) {
-          launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, f.x2, 1, 0, a);
+          launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, f.x2, 0, a);
         });
         continue;
       }
@@ -1279,7 +1214,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     ProfScope ps(lc, kKfAmgUp0, 0.0);
     const int nb = blocks_for(f.n, lc.rowBlocks);
     with_width(f.maxW, [&](auto W) {
-      launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, z, stride, 1, a);
+      launch_rows(lc, nb, k_amg_up<T, W.value>, a.fl, f, e, amg->omega, amg->corr, a.z, 1, a);
     });
   }
 }
@@ -1343,19 +1278,13 @@ cudaError_t amg_capture_graph(const LaunchCfg& lc, const PcgArgsT<T>& a, AmgDevT
 
 // p = z + beta p_old, q = A p of iteration `it` (p0/p1 alternate)
 template <class T>
-static void launch_pq(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, bool il) {
+static void launch_pq(const LaunchCfg& lc, const PcgArgsT<T>& a, int it) {
+  const T* pOld = (it & 1) ? a.p1 : a.p0;
+  T* pNew = (it & 1) ? a.p0 : a.p1;
   // algorithmic bytes: 12 B per off-diagonal (value + column) and 40 B per row in FP64; values
   // and vectors halve in FP32
   const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
   ProfScope ps(lc, kKfPcgSpmv, by);
-  if (il) {  // pairs zp[it & 1] = {z, p_old}; p_new to the p halves of the other pair array
-    const T* zpOld = a.zp[it & 1];
-    T* zpNew = a.zp[(it + 1) & 1];
-    with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq_il<T, W.value>, a, zpOld, zpNew); });
-    return;
-  }
-  const T* pOld = (it & 1) ? a.p1 : a.p0;
-  T* pNew = (it & 1) ? a.p0 : a.p1;
   with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, W.value>, a, pOld, pNew); });
 }
 
@@ -1422,7 +1351,7 @@ static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, A
       lc.stream,
       [&] {
         for (int it = 0; it < 2; ++it) {
-          launch_pq(quiet, a, it, a.zp[0] != nullptr);
+          launch_pq(quiet, a, it);
           vcycle(quiet, a, &amg, (it + 1) & 1);
         }
       },
@@ -1435,8 +1364,7 @@ static cudaError_t pcg_capture_loop(const LaunchCfg& lc, const PcgArgsT<T>& a, A
 template <class T>
 static bool same_pcg_buffers(const PcgArgsT<T>& x, const PcgArgsT<T>& y) {
   return x.A.val == y.A.val && x.A.diag == y.A.diag && x.A.col == y.A.col && x.x == y.x && x.r == y.r &&
-         x.r2 == y.r2 && x.z == y.z && x.p0 == y.p0 && x.p1 == y.p1 && x.zp[0] == y.zp[0] && x.zp[1] == y.zp[1] &&
-         x.q == y.q && x.sc == y.sc &&
+         x.r2 == y.r2 && x.z == y.z && x.p0 == y.p0 && x.p1 == y.p1 && x.q == y.q && x.sc == y.sc &&
          x.fl == y.fl && x.maxit == y.maxit && x.mode == y.mode && x.red.partials == y.red.partials;
 }
 
@@ -1502,7 +1430,7 @@ template <class T>
 void pcg_iteration(const LaunchCfg& lc, const PcgArgsT<T>& a, int it, const AmgDevT<T>* amg) {
   T* pNew = (it & 1) ? a.p0 : a.p1;
   const bool useAmg = amg && amg->nLevels >= 2;
-  launch_pq(lc, a, it, useAmg && a.zp[0] != nullptr);  // the V-cycle path keeps z and p interleaved
+  launch_pq(lc, a, it);
   if (useAmg) {
     // the V-cycle's level-0 sweep applies x += alpha pNew, r -= alpha q: variant (it + 1) & 1 reads
     // the residual this iteration starts from and uses pNew (p1 on even iterations)
