@@ -188,7 +188,6 @@ DSell mom_sell(const anb_ctx* c);
 DSell p_sell(const anb_ctx* c);
 void grad(anb_ctx* c, int nf, const double* const* phi, const unsigned char* bits, double* const* out);
 void poll(anb_ctx* c, const int* dflags, int count);
-void solve_momentum(anb_ctx* c, const int* active, int its[3], bool conv[3]);
 PcgArgs pcg_args(anb_ctx* c, const double* b, double rtol);
 void solve_pressure(anb_ctx* c, const double* b, double* x, double rtol, int* its, bool* conv);
 void ensure_amg(anb_ctx* c);
