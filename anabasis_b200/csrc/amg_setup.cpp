@@ -254,55 +254,4 @@ std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector
   return levels;
 }
 
-int plan_smem_tail_layout(const std::vector<AmgLevelHost>& H, int cluster, size_t valBytes, size_t budget,
-                          int maxLevels, SmemTailLevel* lay, size_t* bytes) {
-  const int L = (int)H.size();
-  int best = 0;
-  *bytes = 0;
-  std::vector<SmemTailLevel> keep;
-  for (int t0 = L - 2; t0 >= 1 && L - t0 <= maxLevels; --t0) {
-    if (!H[t0].sliceOff.empty() || H[t0].n > 65535) break;
-    std::vector<SmemTailLevel> cur(L);
-    size_t off = 0;
-    auto take = [&](size_t n) {
-      const size_t o = off;
-      off += (n + 15) & ~size_t(15);
-      return (int)o;
-    };
-    for (int l = t0; l < L; ++l) {
-      const int n = H[l].n, cs = (n + cluster - 1) / cluster;
-      SmemTailLevel& s = cur[l];
-      s = SmemTailLevel{};
-      s.cs = cs;
-      s.oB = take(valBytes * cs);
-      s.oX = take(valBytes * cs);
-      if (l + 1 == L) continue;  // the dense level holds b and x only
-      const int nn = H[l + 1].n, csn = (nn + cluster - 1) / cluster;
-      int maxE = 0, maxM = 0;
-      for (int r = 0; r < cluster; ++r) {
-        const int r0 = std::min(n, r * cs), r1 = std::min(n, r0 + cs);
-        maxE = std::max(maxE, H[l].rowOff[r1] - H[l].rowOff[r0]);
-        const int I0 = std::min(nn, r * csn), I1 = std::min(nn, I0 + csn);
-        maxM = std::max(maxM, H[l].memOff[I1] - H[l].memOff[I0]);
-      }
-      s.oVal = take(valBytes * maxE);
-      s.oCol = take(2 * (size_t)maxE);
-      s.oColAgg = take(2 * (size_t)maxE);
-      s.oRow = take(4 * (size_t)(cs + 1));
-      s.oDiag = take(valBytes * cs);
-      s.oWd = take(valBytes * cs);
-      s.oAgg = take(2 * (size_t)cs);
-      s.oX2 = take(valBytes * cs);
-      s.oMemOff = take(4 * (size_t)(csn + 1));
-      s.oMem = take(2 * (size_t)maxM);
-    }
-    if (off > budget) break;
-    best = t0;
-    *bytes = off;
-    keep = cur;
-  }
-  for (int l = best; best > 0 && l < L; ++l) lay[l] = keep[l];
-  return best;
-}
-
 }  // namespace anb

@@ -54,19 +54,4 @@ struct AmgSetupOptions {
 std::vector<AmgLevelHost> build_amg_hierarchy(const Layout& L, const std::vector<double>& vals,
                                               const std::vector<double>& diag, const AmgSetupOptions& opt);
 
-// One level of the cluster-resident tail (k_amg_tail_smem): rows per CTA (CTA r owns rows
-// [r cs, (r + 1) cs) and the next level's aggregates [r csNext, ...)) and the byte offsets of the
-// level's arrays in every CTA's dynamic shared memory (the same layout in each CTA).
-struct SmemTailLevel {
-  int cs;
-  int oVal, oCol, oColAgg, oRow, oDiag, oWd, oAgg, oB, oX, oX2, oMemOff, oMem;
-};
-
-// Layout of the cluster-resident tail: the longest run of CSR levels t0..L-2 (plus the dense
-// level L-1) of at most maxLevels levels, with t0 >= 1 and every row count below 65,536, whose
-// per-CTA share for `cluster` CTAs fits `budget` bytes (values of valBytes each).  Returns t0 and
-// fills lay[t0..L-1] and *bytes; 0 when not even the last CSR level fits.
-int plan_smem_tail_layout(const std::vector<AmgLevelHost>& H, int cluster, size_t valBytes, size_t budget,
-                          int maxLevels, SmemTailLevel* lay, size_t* bytes);
-
 }  // namespace anb

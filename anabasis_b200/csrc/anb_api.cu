@@ -375,49 +375,6 @@ constexpr int kAmgFusedDownRows = 65536;
 // beyond); ANB_BLOCKS_PER_SM overrides.
 constexpr int kBlocksPerSM = 8;
 
-// Cluster-resident tail: the longest run of CSR levels ending at the dense level whose per-CTA
-// share (rows split evenly over the cluster's CTAs) fits the shared memory of a CTA, provided it
-// starts no later than the L2-based tail would; every index there must fit 16 bits.  Stores the
-// per-level shared-memory layout and uploads the 16-bit index copies.  ANB_AMG_SMEM_TAIL=0 keeps
-// the L2-based tail.
-template <class T>
-void plan_smem_tail(anb_ctx* c, AmgDevT<T>& A, const std::vector<AmgLevelHost>& H, DevArena& ar) {
-  A.smemTail0 = 0;
-  const char* env = std::getenv("ANB_AMG_SMEM_TAIL");
-  const int L = A.nLevels;
-  if ((env && env[0] == '0') || A.tailRows <= 0 || A.tailCluster <= 0 || L < 3) return;
-  int oldT0 = L - 1;  // first level of the L2-based tail (tail_start in the V-cycle)
-  while (oldT0 - 1 >= 1 && H[oldT0 - 1].n <= A.tailRows && H[oldT0 - 1].sliceOff.empty() && L - (oldT0 - 1) <= 12)
-    --oldT0;
-  for (int cluster : {16, 8}) {
-    SmemTailLevel lay[24] = {};
-    size_t bytes = 0;
-    const int t0 = plan_smem_tail_layout(H, cluster, sizeof(T), kSmemTailMaxBytes, 12, lay, &bytes);
-    if (t0 == 0 || t0 > oldT0) return;
-    if (!amg_smem_tail_fits<T>(cluster, bytes, c->stream)) continue;
-    for (int l = t0; l + 1 < L; ++l) {
-      const AmgLevelHost& h = H[l];
-      std::vector<unsigned short> col16(h.col.size()), colAgg16(h.col.size()), agg16(h.agg.size()),
-          mem16(h.mem.size());
-      for (size_t k = 0; k < h.col.size(); ++k) {
-        col16[k] = (unsigned short)h.col[k];
-        colAgg16[k] = (unsigned short)h.agg[h.col[k]];
-      }
-      for (size_t i = 0; i < h.agg.size(); ++i) agg16[i] = (unsigned short)h.agg[i];
-      for (size_t m = 0; m < h.mem.size(); ++m) mem16[m] = (unsigned short)h.mem[m];
-      A.lv[l].col16 = ar.upload(col16);
-      A.lv[l].colAgg16 = ar.upload(colAgg16);
-      A.lv[l].agg16 = ar.upload(agg16);
-      A.lv[l].mem16 = ar.upload(mem16);
-    }
-    A.smemTail0 = t0;
-    A.smemCluster = cluster;
-    A.smemBytes = bytes;
-    std::copy(lay, lay + 24, A.smLayout);
-    return;
-  }
-}
-
 // Aggregation hierarchy for the current level-0 matrix (val0/diag0 on the device, storage type T),
 // coarse levels in T, coarsest inverse in double, host structure in H, device arrays in ar.  For the
 // pressure hierarchy (ga != nullptr) the PCG V-cycles are captured as graphs for *ga.
@@ -494,15 +451,13 @@ void build_amg(anb_ctx* c, AmgDevT<T>& A, std::vector<AmgLevelHost>& H, DevArena
   amg_configure_tail(A, tailEnv ? std::atoi(tailEnv) : kAmgTailRows, c->stream);
   const char* fdEnv = std::getenv("ANB_AMG_FUSED_DOWN_ROWS");
   A.fusedDownRows = fdEnv ? std::atoi(fdEnv) : kAmgFusedDownRows;
-  plan_smem_tail(c, A, H, ar);
   const char* verbose = std::getenv("ANB_AMG_VERBOSE");
   if (verbose && verbose[0] == '1') {
     std::fprintf(stderr, "AMG levels (rows/stored entries/max width):");
     for (int l = 0; l < A.nLevels; ++l)
       std::fprintf(stderr, " %d/%lld/%d", A.lv[l].n, l == 0 ? (long long)c->nEnt : (long long)H[l].nStore,
                    l == 0 ? c->L.maxRowLen : H[l].maxW);
-    std::fprintf(stderr, " | tail rows %d, cluster %d | shared-memory tail from level %d, %d CTAs, %zu B each\n",
-                 A.tailRows, A.tailCluster, A.smemTail0, A.smemCluster, A.smemBytes);
+    std::fprintf(stderr, " | tail rows %d, cluster %d\n", A.tailRows, A.tailCluster);
   }
   const char* noGraph = std::getenv("ANB_NO_GRAPH");
   if (ga && A.nLevels >= 2 && !(noGraph && noGraph[0] == '1')) CK(amg_capture_graph(c->lc, *ga, A));

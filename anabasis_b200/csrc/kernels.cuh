@@ -1,7 +1,6 @@
 // Launch wrappers for the SIMPLE kernels (implemented in kernels.cu).
 #pragma once
 
-#include "amg_setup.hpp"
 #include "device.cuh"
 
 #include <atomic>
@@ -317,9 +316,6 @@ struct AmgLevelDevT {
   // member mem[m] per member slot m; they take one dependent load out of the up and down sweeps
   const int* colAgg;
   const int2* memRow;
-  // levels of the cluster-resident tail (k_amg_tail_smem): 16-bit copies of col, colAgg, agg and
-  // mem (every index there is below 65,536), staged into shared memory with the values
-  const unsigned short *col16, *colAgg16, *agg16, *mem16;
   const int* gOff;     // Galerkin gather for the next level's storage
   const int* gIdx;
   int nEntNext;        // next level's SELL storage entries
@@ -352,12 +348,6 @@ struct AmgDevT {
   // thread-block-cluster kernel of tailCluster CTAs (0: one launch per level and sweep).
   int tailRows = 0;
   int tailCluster = 0;
-  // Cluster-resident tail (plan_smem_tail): levels smemTail0..nLevels-1 staged into the distributed
-  // shared memory of one cluster of smemCluster CTAs (smemTail0 = 0: not used)
-  int smemTail0 = 0;
-  int smemCluster = 0;
-  size_t smemBytes = 0;
-  SmemTailLevel smLayout[24] = {};
   // CSR levels of at most this many rows (above the tail) run their down sweep and restriction
   // as one kernel, warp per aggregate (same values; fewer launches, longer chains per warp)
   int fusedDownRows = 0;
@@ -401,11 +391,6 @@ void amg_release_graphs(AmgDevT<T>& amg);
 // cluster size for this device.  Call before amg_capture_graph.
 template <class T>
 void amg_configure_tail(AmgDevT<T>& amg, int tailRows, cudaStream_t s);
-// Whether one cluster of `cluster` CTAs of the cluster-resident tail kernel with `bytes` of dynamic
-// shared memory each can be resident on this device (sets the kernel's attributes).
-constexpr size_t kSmemTailMaxBytes = 227 * 1024;  // dynamic shared memory per CTA, the sm_100 maximum
-template <class T>
-bool amg_smem_tail_fits(int cluster, size_t bytes, cudaStream_t s);
 
 // ---- mixed-precision defect correction (FP64 outer residual around FP32 inner solves) ------
 // r = b - A x in double with the float matrix, r32 = r, per-component |r|^2 and |b|^2 in

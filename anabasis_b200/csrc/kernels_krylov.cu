@@ -857,193 +857,6 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_amg_tail(const int* done, c
   }
 }
 
-// ---- cluster-resident coarse tail ----------------------------------------------------------
-// The CSR levels from smemTail0 on and the dense level as one cluster kernel whose data live in
-// the cluster's distributed shared memory: CTA r stages the rows it owns (values, 16-bit column and
-// aggregate indices, diagonal, smoother weights) and the member lists of the next level's
-// aggregates it owns; each sweep then reads its own rows from its shared memory and the
-// neighbours' vector entries from the owning CTA's (DSMEM), with a cluster barrier between sweeps
-// and no global-memory round trip inside the launch.  Rows, sums and their order are those of
-// resid_csr_rows, restrict_rows, dense_rows and up_csr_rows, so the values equal k_amg_tail's bit for
-// bit.  Only the first level's right-hand side comes from global memory and only its smoothed
-// solution (x2, the correction of the level above) goes back.  tests/native/smem_tail_check.cpp
-// replays the indexing of this kernel on the CPU with bounds checks.
-template <class T>
-struct SmemTailArgs {
-  int nLev;
-  AmgLevelDevT<T> lv[kTailMaxLevels];
-  SmemTailLevel sm[kTailMaxLevels];
-  const double* dense;
-  double corr;
-};
-
-// A level vector partitioned cs entries per CTA, at the same shared-memory offset in every CTA.
-template <class T>
-struct DsmVec {
-  T* base;  // this CTA's part
-  int cs;
-  __device__ __forceinline__ double get(const cg::cluster_group& cl, int j) const {
-    const int r = j / cs;
-    return (double)*cl.map_shared_rank(base + (j - r * cs), r);
-  }
-};
-
-template <class T>
-__global__ void __launch_bounds__(kTailThreads, 1) k_amg_tail_smem(const int* done,
-                                                                   const __grid_constant__ SmemTailArgs<T> a) {
-  if (*done) return;  // uniform over the cluster: no CTA waits for one that left
-  extern __shared__ __align__(16) unsigned char smem[];
-  cg::cluster_group cl = cg::this_cluster();
-  const int rank = (int)cl.block_rank();
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5, nWarps = nt >> 5;
-  constexpr int G = kCoarseLanes, RPW = 32 / G;
-  const int L = a.nLev;
-  auto at = [&](int off) { return smem + off; };
-  // 1. staging: this CTA's rows of every level (coalesced copies, all independent)
-  for (int l = 0; l < L; ++l) {
-    const AmgLevelDevT<T>& f = a.lv[l];
-    const SmemTailLevel& s = a.sm[l];
-    const int r0 = min(f.n, rank * s.cs), nl = min(f.n, r0 + s.cs) - r0;
-    if (l == 0) {
-      T* sb = reinterpret_cast<T*>(at(s.oB));
-      for (int i = tid; i < nl; i += nt) sb[i] = f.b[r0 + i];
-    }
-    if (l + 1 == L) break;  // the dense level holds vectors only
-    const int e0 = __ldg(&f.rowOff[r0]), ne = __ldg(&f.rowOff[r0 + nl]) - e0;
-    T* sval = reinterpret_cast<T*>(at(s.oVal));
-    unsigned short* scol = reinterpret_cast<unsigned short*>(at(s.oCol));
-    unsigned short* scag = reinterpret_cast<unsigned short*>(at(s.oColAgg));
-    for (int k = tid; k < ne; k += nt) {
-      sval[k] = __ldg(&f.val[e0 + k]);
-      scol[k] = __ldg(&f.col16[e0 + k]);
-      scag[k] = __ldg(&f.colAgg16[e0 + k]);
-    }
-    int* srow = reinterpret_cast<int*>(at(s.oRow));
-    T* sd = reinterpret_cast<T*>(at(s.oDiag));
-    T* swd = reinterpret_cast<T*>(at(s.oWd));
-    unsigned short* sagg = reinterpret_cast<unsigned short*>(at(s.oAgg));
-    for (int i = tid; i <= nl; i += nt) {
-      srow[i] = __ldg(&f.rowOff[r0 + i]) - e0;
-      if (i < nl) {
-        sd[i] = __ldg(&f.diag[r0 + i]);
-        swd[i] = __ldg(&f.wdinv[r0 + i]);
-        sagg[i] = __ldg(&f.agg16[r0 + i]);
-      }
-    }
-    const SmemTailLevel& sn = a.sm[l + 1];
-    const int nNext = a.lv[l + 1].n;
-    const int I0 = min(nNext, rank * sn.cs), nI = min(nNext, I0 + sn.cs) - I0;
-    const int m0 = __ldg(&f.memOff[I0]), nm = __ldg(&f.memOff[I0 + nI]) - m0;
-    int* smo = reinterpret_cast<int*>(at(s.oMemOff));
-    unsigned short* smm = reinterpret_cast<unsigned short*>(at(s.oMem));
-    for (int I = tid; I <= nI; I += nt) smo[I] = __ldg(&f.memOff[I0 + I]) - m0;
-    for (int m = tid; m < nm; m += nt) smm[m] = __ldg(&f.mem16[m0 + m]);
-  }
-  cl.sync();
-  // 2. down: x = w D^-1 b, x2 = b - A x on the own rows, then the own aggregates' b of the next level
-  for (int l = 0; l + 1 < L; ++l) {
-    const AmgLevelDevT<T>& f = a.lv[l];
-    const SmemTailLevel& s = a.sm[l];
-    const int r0 = min(f.n, rank * s.cs), nl = min(f.n, r0 + s.cs) - r0;
-    const T* sval = reinterpret_cast<const T*>(at(s.oVal));
-    const unsigned short* scol = reinterpret_cast<const unsigned short*>(at(s.oCol));
-    const int* srow = reinterpret_cast<const int*>(at(s.oRow));
-    T* sb = reinterpret_cast<T*>(at(s.oB));
-    T* swd = reinterpret_cast<T*>(at(s.oWd));
-    const T* sd = reinterpret_cast<const T*>(at(s.oDiag));
-    T* sx = reinterpret_cast<T*>(at(s.oX));
-    T* sx2 = reinterpret_cast<T*>(at(s.oX2));
-    const DsmVec<T> vb{sb, s.cs}, vwd{swd, s.cs};
-    for (int base = warp * RPW; base < nl; base += nWarps * RPW) {  // bound uniform over the warp
-      const int i = base + lane / G, sub = lane % G;
-      double acc = 0.0;
-      if (i < nl) {
-        const int k1 = srow[i + 1];
-        for (int k = srow[i] + sub; k < k1; k += G) {
-          const int j = scol[k];
-          acc += (double)sval[k] * (vwd.get(cl, j) * vb.get(cl, j));
-        }
-      }
-      acc = group_sum<G>(acc);
-      if (i < nl && sub == 0) {
-        const double di = (double)sd[i], bi = (double)sb[i];
-        const double xi = (double)swd[i] * bi;
-        sx[i] = (T)xi;
-        sx2[i] = (T)(bi - di * xi - acc);
-      }
-    }
-    cl.sync();
-    const SmemTailLevel& sn = a.sm[l + 1];
-    const int nNext = a.lv[l + 1].n;
-    const int I0 = min(nNext, rank * sn.cs), nI = min(nNext, I0 + sn.cs) - I0;
-    const int* smo = reinterpret_cast<const int*>(at(s.oMemOff));
-    const unsigned short* smm = reinterpret_cast<const unsigned short*>(at(s.oMem));
-    T* sbn = reinterpret_cast<T*>(at(sn.oB));
-    const DsmVec<T> vx2{sx2, s.cs};
-    for (int I = tid; I < nI; I += nt) {
-      double acc = 0.0;
-      const int m1 = smo[I + 1];
-      for (int m = smo[I]; m < m1; ++m) acc += vx2.get(cl, smm[m]);
-      sbn[I] = (T)acc;
-    }
-    cl.sync();
-  }
-  // 3. coarsest level: x = A^-1 b with the stored dense inverse, warp per own row
-  {
-    const AmgLevelDevT<T>& f = a.lv[L - 1];
-    const SmemTailLevel& s = a.sm[L - 1];
-    const int r0 = min(f.n, rank * s.cs), nl = min(f.n, r0 + s.cs) - r0;
-    const DsmVec<T> vb{reinterpret_cast<T*>(at(s.oB)), s.cs};
-    T* sx = reinterpret_cast<T*>(at(s.oX));
-    for (int i = warp; i < nl; i += nWarps) {
-      double acc = 0.0;
-      for (int j = lane; j < f.n; j += 32) acc += __ldg(&a.dense[(size_t)(r0 + i) * f.n + j]) * vb.get(cl, j);
-      acc = warp_sum(acc);
-      if (lane == 0) sx[i] = (T)acc;
-    }
-  }
-  // 4. up: prolongate the coarser correction and post-smooth, finest tail level last (to global)
-  for (int l = L - 2; l >= 0; --l) {
-    cl.sync();
-    const AmgLevelDevT<T>& f = a.lv[l];
-    const SmemTailLevel& s = a.sm[l];
-    const SmemTailLevel& sn = a.sm[l + 1];
-    const int r0 = min(f.n, rank * s.cs), nl = min(f.n, r0 + s.cs) - r0;
-    const T* sval = reinterpret_cast<const T*>(at(s.oVal));
-    const unsigned short* scol = reinterpret_cast<const unsigned short*>(at(s.oCol));
-    const unsigned short* scag = reinterpret_cast<const unsigned short*>(at(s.oColAgg));
-    const unsigned short* sagg = reinterpret_cast<const unsigned short*>(at(s.oAgg));
-    const int* srow = reinterpret_cast<const int*>(at(s.oRow));
-    const T* sb = reinterpret_cast<const T*>(at(s.oB));
-    const T* swd = reinterpret_cast<const T*>(at(s.oWd));
-    const T* sd = reinterpret_cast<const T*>(at(s.oDiag));
-    T* sx = reinterpret_cast<T*>(at(s.oX));
-    T* sx2 = reinterpret_cast<T*>(at(s.oX2));
-    // correction from the coarser level: its smoothed solution (x2), or x on the coarsest
-    T* ebase = reinterpret_cast<T*>(at(l + 1 == L - 1 ? sn.oX : sn.oX2));
-    const DsmVec<T> vx{sx, s.cs}, ve{ebase, sn.cs};
-    for (int base = warp * RPW; base < nl; base += nWarps * RPW) {
-      const int i = base + lane / G, sub = lane % G;
-      double acc = 0.0;
-      if (i < nl) {
-        const int k1 = srow[i + 1];
-        for (int k = srow[i] + sub; k < k1; k += G)
-          acc += (double)sval[k] * (vx.get(cl, scol[k]) + a.corr * ve.get(cl, scag[k]));
-      }
-      acc = group_sum<G>(acc);
-      if (i < nl && sub == 0) {
-        const double di = (double)sd[i];
-        const double xi = (double)sx[i] + a.corr * ve.get(cl, sagg[i]);
-        const T o = (T)(xi + (double)swd[i] * ((double)sb[i] - di * xi - acc));
-        if (l == 0) f.x2[r0 + i] = o;
-        else sx2[i] = o;
-      }
-    }
-  }
-  cl.sync();  // no CTA leaves while another may still read its shared memory
-}
-
 // Galerkin values of the next level: one gather list per coarse storage entry (sums in double).
 template <class T>
 __global__ void __launch_bounds__(kBlock) k_amg_galerkin(AmgLevelDevT<T> f, T* valNext, T* diagNext, T* wdinvNext,
@@ -1313,45 +1126,6 @@ static void launch_tail(const LaunchCfg& lc, const int* done, const AmgDevT<T>* 
   cudaLaunchKernelEx(&cfg, k_amg_tail<T>, done, ta);
 }
 
-template <class T>
-static void launch_smem_tail(const LaunchCfg& lc, const int* done, const AmgDevT<T>* amg) {
-  SmemTailArgs<T> ta{};
-  const int t0 = amg->smemTail0;
-  ta.nLev = amg->nLevels - t0;
-  for (int l = 0; l < ta.nLev; ++l) {
-    ta.lv[l] = amg->lv[t0 + l];
-    ta.sm[l] = amg->smLayout[t0 + l];
-  }
-  ta.dense = amg->dense;
-  ta.corr = amg->corr;
-  cudaLaunchAttribute at[1];
-  cudaLaunchConfig_t cfg = tail_config(lc.stream, amg->smemCluster, at);
-  cfg.dynamicSmemBytes = amg->smemBytes;
-  cudaLaunchKernelEx(&cfg, k_amg_tail_smem<T>, done, ta);
-}
-
-template <class T>
-bool amg_smem_tail_fits(int cluster, size_t bytes, cudaStream_t s) {
-  // the attribute allows the whole budget, so that hierarchies planned with different sizes can
-  // all launch the kernel
-  if (bytes > kSmemTailMaxBytes ||
-      cudaFuncSetAttribute(k_amg_tail_smem<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
-      cudaFuncSetAttribute(k_amg_tail_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemTailMaxBytes) !=
-          cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  cudaLaunchAttribute at[1];
-  cudaLaunchConfig_t cfg = tail_config(s, cluster, at);
-  cfg.dynamicSmemBytes = bytes;
-  int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, k_amg_tail_smem<T>, &cfg) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return n > 0;
-}
-
 // Cluster size of the tail: 16 CTAs (a non-portable size) when the device can co-schedule them,
 // else 8; 0 (no tail) when neither fits.
 template <class T>
@@ -1391,8 +1165,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
     k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[1].b);
   }
   {
-    const bool smemTail = amg->smemTail0 > 0;
-    const int t0 = smemTail ? amg->smemTail0 : tail_start(amg);
+    const int t0 = tail_start(amg);
     auto fused = [&](const AmgLevelDevT<T>& f) { return !f.sliceOff && f.n <= amg->fusedDownRows; };
     int nl = 1;
     for (int l = 1; l < t0; ++l) nl += fused(amg->lv[l]) ? 2 : 3;
@@ -1414,9 +1187,7 @@ static void vcycle(const LaunchCfg& lc, const PcgArgsT<T>& a, const AmgDevT<T>* 
           a.fl, f, amg->omega);
       k_amg_restrict<T><<<blocks_for(f.nc, lc.rowBlocks), kBlock, 0, lc.stream>>>(a.fl, f, amg->lv[l + 1].b);
     }
-    if (smemTail) {
-      launch_smem_tail(lc, a.fl, amg);
-    } else if (t0 < L - 1) {
+    if (t0 < L - 1) {
       launch_tail(lc, a.fl, amg, t0);
     } else {
       const AmgLevelDevT<T>& c = amg->lv[L - 1];
@@ -1748,7 +1519,6 @@ void launch_apply_correction(const LaunchCfg& lc, int n, int nc, double* x, floa
   template bool bicg_loop_launch<T>(const LaunchCfg&, const BicgArgsT<T>&, BicgLoopT<T>&);     \
   template void bicg_loop_release<T>(BicgLoopT<T>&);                                          \
   template void amg_configure_tail<T>(AmgDevT<T>&, int, cudaStream_t);                          \
-  template bool amg_smem_tail_fits<T>(int, size_t, cudaStream_t);                               \
   template void amg_apply<T>(const LaunchCfg&, const PcgArgsT<T>&, const AmgDevT<T>*, cudaGraphExec_t*); \
   template void bicg_iteration_precond<T>(const LaunchCfg&, const BicgArgsT<T>&, void (*)(void*, int, int), void*);
 ANB_INSTANTIATE(double)

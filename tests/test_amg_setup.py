@@ -26,23 +26,3 @@ def checker(tmp_path_factory):
 def test_sell_and_csr_coarse_levels_agree(checker, dims):
     r = subprocess.run([str(checker), *map(str, dims)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip().endswith("OK"), r.stdout + r.stderr
-
-
-@pytest.fixture(scope="module")
-def tail_checker(tmp_path_factory):
-    if shutil.which("g++") is None:
-        pytest.skip("g++ not available")
-    exe = tmp_path_factory.mktemp("tail") / "smem_tail_check"
-    src = ROOT / "anabasis_b200" / "csrc"
-    subprocess.run(["g++", "-O2", "-std=c++17", f"-I{src}", str(ROOT / "tests" / "native" / "smem_tail_check.cpp"),
-                    str(src / "amg_setup.cpp"), "-o", str(exe)], check=True)
-    return exe
-
-
-@pytest.mark.parametrize("dims", [(120, 60, 40, 16), (60, 25, 24, 16), (60, 25, 24, 8), (24, 10, 10, 16)])
-def test_cluster_resident_tail_layout_and_replay(tail_checker, dims):
-    """The shared-memory layout of the cluster-resident AMG tail, replayed on the CPU: every staged
-    and swept index stays inside its array, no entry is read before it is written, and the result
-    equals the whole-level V-cycle tail bit for bit (tests/native/smem_tail_check.cpp)."""
-    r = subprocess.run([str(tail_checker), *map(str, dims)], capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0 and r.stdout.strip().endswith("OK"), r.stdout + r.stderr

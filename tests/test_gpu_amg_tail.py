@@ -78,32 +78,3 @@ def test_sell_coarse_levels_match_csr(precision):
     tol = 1e-7 if precision == 0 else 1e-5  # the mixed method's FP32 inner solves round differently
     for k in ("u", "v", "w"):
         assert np.abs(got[k] - ref[k]).max() <= tol * scale, k
-
-
-@pytest.mark.parametrize("precision", [0, 1])
-def test_cluster_resident_tail_is_bit_identical(precision, capfd):
-    """The coarse tail held in the distributed shared memory of one cluster (k_amg_tail_smem) does the
-    L2-based tail's arithmetic in the same order: same fields and iteration counts as with
-    ANB_AMG_SMEM_TAIL=0, and the hierarchy really ran it (ANB_AMG_VERBOSE reports its first level)."""
-    m, bc, _ = channel(nx=60, ny=25, nz=24, jitter=0.15, seed=3, obstacle=True)
-    init = initial_state(m, bc)
-    old = {k: os.environ.get(k) for k in ("ANB_AMG_SMEM_TAIL", "ANB_AMG_VERBOSE")}
-    try:
-        os.environ["ANB_AMG_SMEM_TAIL"] = "0"
-        ref, st0 = _run(m, bc, init, precision, 1024, 65536)
-        os.environ.pop("ANB_AMG_SMEM_TAIL")
-        os.environ["ANB_AMG_VERBOSE"] = "1"
-        capfd.readouterr()
-        got, st = _run(m, bc, init, precision, 1024, 65536)
-        err = capfd.readouterr().err
-    finally:
-        for k, v in old.items():
-            if v is None:
-                os.environ.pop(k, None)
-            else:
-                os.environ[k] = v
-    line = [x for x in err.splitlines() if "shared-memory tail from level" in x]
-    assert line and " from level 0," not in line[0], err
-    assert [x["its_p_total"] for x in st] == [x["its_p_total"] for x in st0]
-    for k in ("u", "v", "w", "p", "phi"):
-        assert np.array_equal(got[k], ref[k]), k
