@@ -987,140 +987,6 @@ __global__ void __launch_bounds__(1024, 1) k_amg_dense_factor(AmgLevelDevT<T> c,
     }
 }
 
-// The same inverse by blocked Gauss-Jordan: the pivots in blocks of 32, so that a block costs four
-// barriers instead of 32.  For pivot block K (rows/columns kb..kb+nb-1), with R = A[K, :] and
-// C = A[:, K] taken before the step:
-//   warp 0 inverts P = A[K, K] in shared memory by the textbook steps above (same skip rule), then
-//   A[K, K] = P^-1,  A[K, j] = W[:, j] = P^-1 R[:, j],  A[i, K] = -C[i, :] P^-1,
-//   A[i, j] -= C[i, :] W[:, j]  (i, j outside K).
-// This is the unblocked elimination regrouped, so the inverse agrees to rounding (and a skipped
-// pivot zeroes the same row and column).  Shared memory: the n x n assembly area, reused for
-// R and W (32 x 32 NC each), C (32 NC x 32) and P (32 x 32).
-template <class T, int NC>
-__global__ void __launch_bounds__(1024, 1) k_amg_dense_inv(AmgLevelDevT<T> c, double* inv) {
-  extern __shared__ double A[];
-  __shared__ double colk[32], rowk[32];
-  __shared__ double dmax;
-  constexpr int NCOL = 32 * NC;
-  const int n = c.n;
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) A[t] = 0.0;
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {  // the coarsest level is always CSR
-    A[i * n + i] = (double)c.diag[i];
-    for (int k = c.rowOff[i]; k < c.rowOff[i + 1]; ++k) {
-      const int j = c.col[k];
-      if (j != i) A[i * n + j] += (double)c.val[k];
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double mx = 0.0;
-    for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(A[i * n + i]));
-    dmax = mx;
-  }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double a[NC][NC];
-#pragma unroll
-  for (int p = 0; p < NC; ++p)
-#pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      const int i = w + 32 * p, j = lane + 32 * q;
-      a[p][q] = (i < n && j < n) ? A[i * n + j] : 0.0;
-    }
-  __syncthreads();
-  const double dm = dmax;
-  double* R = A;                // [32][NCOL]
-  double* W = R + 32 * NCOL;    // [32][NCOL]
-  double* Cb = W + 32 * NCOL;   // [NCOL][32]
-  double* P = Cb + NCOL * 32;   // [32][32]
-#pragma unroll
-  for (int kc = 0; kc < NC; ++kc) {
-    const int kb = 32 * kc, nb = min(32, n - kb);
-    if (nb <= 0) break;  // uniform over the block
-    // 1. row block and column block (before the step) to shared memory
-    if (w < nb) {
-#pragma unroll
-      for (int q = 0; q < NC; ++q) R[w * NCOL + lane + 32 * q] = a[kc][q];
-    }
-    if (lane < nb) {
-#pragma unroll
-      for (int p = 0; p < NC; ++p) Cb[(w + 32 * p) * 32 + lane] = a[p][kc];
-    }
-    __syncthreads();
-    // 2. warp 0 inverts the pivot block; lane l owns column l
-    if (w == 0) {
-      for (int m = 0; m < 32; ++m) P[m * 32 + lane] = (m < nb && lane < nb) ? R[m * NCOL + kb + lane] : 0.0;
-      __syncwarp();
-      for (int k = 0; k < nb; ++k) {
-        const double piv = P[k * 32 + k];
-        const bool skip = fabs(piv) <= 1e-13 * dm;
-        if (lane < nb) {
-          colk[lane] = P[lane * 32 + k];
-          rowk[lane] = lane == k ? 1.0 / piv : P[k * 32 + lane] / piv;
-        }
-        __syncwarp();
-        if (lane < nb) {
-          const double rl = rowk[lane], rkk = rowk[k];
-          for (int m = 0; m < nb; ++m) {
-            double& e = P[m * 32 + lane];
-            if (skip) {
-              if (m == k || lane == k) e = 0.0;
-            } else if (m == k) {
-              e = rl;
-            } else if (lane == k) {
-              e = -colk[m] * rkk;
-            } else {
-              e = e - colk[m] * rl;
-            }
-          }
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    // 3. W = P^-1 R: warp w < nb forms row w
-    if (w < nb) {
-#pragma unroll
-      for (int q = 0; q < NC; ++q) {
-        const int j = lane + 32 * q;
-        double s = 0.0;
-        for (int t = 0; t < nb; ++t) s += P[w * 32 + t] * R[t * NCOL + j];
-        W[w * NCOL + j] = s;
-      }
-    }
-    __syncthreads();
-    // 4. every owned entry takes its block formula
-#pragma unroll
-    for (int p = 0; p < NC; ++p)
-#pragma unroll
-      for (int q = 0; q < NC; ++q) {
-        const int i = w + 32 * p, j = lane + 32 * q;
-        if (i >= n || j >= n) continue;
-        if (p == kc && q == kc) {
-          a[p][q] = P[w * 32 + lane];
-        } else if (p == kc) {
-          a[p][q] = W[w * NCOL + j];
-        } else if (q == kc) {
-          double s = 0.0;
-          for (int t = 0; t < nb; ++t) s += Cb[i * 32 + t] * P[t * 32 + lane];
-          a[p][q] = -s;
-        } else {
-          double s = 0.0;
-          for (int t = 0; t < nb; ++t) s += Cb[i * 32 + t] * W[t * NCOL + j];
-          a[p][q] -= s;
-        }
-      }
-    __syncthreads();  // R, W, C and P are rewritten by the next block
-  }
-#pragma unroll
-  for (int p = 0; p < NC; ++p)
-#pragma unroll
-    for (int q = 0; q < NC; ++q) {
-      const int i = w + 32 * p, j = lane + 32 * q;
-      if (i < n && j < n) inv[(size_t)i * n + j] = a[p][q];
-    }
-}
-
 // ---------------------------------------------------------------- mixed-precision defect
 // r = b - A x in double (float matrix, double x), r32 = r; per component |r|^2, |b|^2.
 __global__ void __launch_bounds__(kBlock) k_defect(DefectArgs a) {
@@ -1611,31 +1477,18 @@ void amg_refresh(const LaunchCfg& lc, AmgDevT<T>& amg) {
                                                                                              c.wdinv, amg.omega);
   }
   const AmgLevelDevT<T>& c = amg.lv[amg.nLevels - 1];
+  const size_t smem = sizeof(double) * (size_t)c.n * c.n;
   g_launches += 1;
   const int nc = (c.n + 31) / 32;
-  static const bool unblocked = [] {
-    const char* s = std::getenv("ANB_DENSE_UNBLOCKED");
-    return s && s[0] == '1';
-  }();
-  // blocked: the assembly area or the four block buffers, whichever is larger
-  const size_t smem = sizeof(double) * std::max((size_t)c.n * c.n, unblocked ? 0 : 3 * 32 * 32 * (size_t)nc + 1024);
   auto go = [&](auto kern) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     kern<<<1, 1024, smem, lc.stream>>>(c, amg.dense);
   };
-  if (unblocked) {
-    if (nc <= 1) go(k_amg_dense_factor<T, 1>);
-    else if (nc == 2) go(k_amg_dense_factor<T, 2>);
-    else if (nc == 3) go(k_amg_dense_factor<T, 3>);
-    else if (nc == 4) go(k_amg_dense_factor<T, 4>);
-    else go(k_amg_dense_factor<T, 5>);
-    return;
-  }
-  if (nc <= 1) go(k_amg_dense_inv<T, 1>);
-  else if (nc == 2) go(k_amg_dense_inv<T, 2>);
-  else if (nc == 3) go(k_amg_dense_inv<T, 3>);
-  else if (nc == 4) go(k_amg_dense_inv<T, 4>);
-  else go(k_amg_dense_inv<T, 5>);
+  if (nc <= 1) go(k_amg_dense_factor<T, 1>);
+  else if (nc == 2) go(k_amg_dense_factor<T, 2>);
+  else if (nc == 3) go(k_amg_dense_factor<T, 3>);
+  else if (nc == 4) go(k_amg_dense_factor<T, 4>);
+  else go(k_amg_dense_factor<T, 5>);
 }
 
 void launch_defect(const LaunchCfg& lc, const DefectArgs& a) {
