@@ -39,11 +39,11 @@ sys.path.insert(0, str(ROOT))
 WORKLOAD = dict(nx=200, ny=70, nz=70, jitter=0.15, seed=0, obstacle=True)
 PARAMS = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3, n_nonorth_corr=2)
 KERNEL_FAMILY = 7  # ANB_KF_PCG_SPMV: the largest bandwidth-bound kernel of the step
-# DRAM bytes (read + write) per k_pcg_pq launch on this workload: mean of 3 launches of
-#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
-#       -k regex:k_pcg_pq -s 30 -c 3 python bench.py --steps 2 --warmup 3 --no-cpu
-# (93.10 MB read + 3.18 MB write)
-PCG_SPMV_TRAFFIC_BYTES = 96.29e6
+# DRAM bytes (read + write) per k_pcg_pq launch on this workload, from one launch of
+#   ANB_NO_LOOP_GRAPH=1 ncu --set full --clock-control none -k regex:"^k_pcg_pq$" -s 30 -c 1
+#       python bench.py --steps 2 --warmup 3 --no-cpu
+# (93.07 MB read + 6.14 MB write)
+PCG_SPMV_TRAFFIC_BYTES = 99.21e6
 FAMILY_NAMES = {1: "k_lsq_grad", 2: "k_momentum", 3: "k_pressure_rc", 4: "k_nonorth_rhs", 5: "k_flux_final",
                 6: "k_bicg_v/k_bicg_t", 7: "k_pcg_pq"}
 
