@@ -110,6 +110,7 @@ SIGNATURES = {
     "anb_debug_momentum": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "anb_debug_pressure": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp]),
     "anb_debug_pressure_solve": (ct.c_int, [ct.c_void_p, _dp, _dp, _ip, _dp]),
+    "anb_debug_nonorth": (ct.c_int, [ct.c_void_p, _dp, _dp, _dp, _dp, _dp]),
     "anb_mesh_read_polymesh": (ct.c_int, [ct.c_char_p, ct.POINTER(ct.c_void_p), ct.c_char_p, ct.c_int]),
     "anb_mesh_make_channel": (ct.c_int, [ct.c_int, ct.c_int, ct.c_int, ct.c_double, ct.c_double, ct.c_double,
                                           ct.c_double, ct.c_ulonglong, ct.c_int, ct.c_int,
@@ -424,6 +425,14 @@ class Solver:
         self._check(lib().anb_debug_pressure(self._h, *map(_d, arrs), _d(o["diag"]), _d(o["a_pn"]),
                                              _d(o["phi_star"]), _d(o["div_star"])))
         return o
+
+    def debug_nonorth(self, rau, grad) -> np.ndarray:
+        """Divergence of the non-orthogonal correction flux for rAU and grad p' (3 x nCells)."""
+        g = np.ascontiguousarray(np.asarray(grad, np.float64).reshape(3, -1))
+        rau = np.ascontiguousarray(rau, np.float64)
+        div = np.zeros(self.n_cells)
+        self._check(lib().anb_debug_nonorth(self._h, _d(rau), _d(g[0]), _d(g[1]), _d(g[2]), _d(div)))
+        return div
 
     def debug_pressure_solve(self, b, x0) -> tuple[np.ndarray, int, float]:
         b = np.ascontiguousarray(b, np.float64)

@@ -1722,6 +1722,29 @@ int anb_debug_pressure(anb_ctx* c, const double* u, const double* v, const doubl
   });
 }
 
+int anb_debug_nonorth(anb_ctx* c, const double* rau, const double* gx, const double* gy, const double* gz,
+                      double* div_no) {
+  if (!c || !div_no) return ANB_ERR_INVALID;
+  return guarded(c, [&]() -> int {
+    if (c->mixed) throw AnbError(ANB_ERR_UNSUPPORTED, "this entry point needs an FP64 (ANB_PRECISION_FP64) context");
+    if (!c->bcSet) throw AnbError(ANB_ERR_INVALID, "boundary conditions not set");
+    CK(cudaSetDevice(c->prm.device));
+    const int C = c->C;
+    const double* s1[1] = {rau};
+    upload_cells(c, s1, c->rau, 1);
+    const double* s3[3] = {gx, gy, gz};
+    upload_cells(c, s3, c->Gc, 3);
+    // b = -divBase + div(phi_NO): with a zero base the right-hand side is the divergence itself
+    CK(cudaMemsetAsync(c->divCorr, 0, sizeof(double) * C, c->stream));
+    NonOrthArgs na{c->rau, c->Gc, c->divCorr, c->pb};
+    launch_nonorth_rhs(c->lc, c->dm, na);
+    CK(cudaGetLastError());
+    double* d1[1] = {div_no};
+    download_cells(c, c->pb, d1, 1);
+    return ANB_OK;
+  });
+}
+
 int anb_debug_pressure_solve(anb_ctx* c, const double* b, double* x, int* iters, double* final_res) {
   if (!c) return ANB_ERR_INVALID;
   return guarded(c, [&]() -> int {

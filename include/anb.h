@@ -291,6 +291,12 @@ int anb_debug_momentum(anb_ctx* ctx, const double* u, const double* v, const dou
 int anb_debug_pressure(anb_ctx* ctx, const double* u, const double* v, const double* w, const double* p,
                        const double* rau, double* diag, double* a_pn, double* phi_star, double* div_star);
 
+/* Divergence of the explicit non-orthogonal correction flux (kernel_pressure_nonorth_flux_and_
+ * divergence, main.cu:1538-1593) for rAU and the gradient (gx, gy, gz) of the pressure
+ * correction; internal faces and the Dirichlet-pressure boundary faces contribute. */
+int anb_debug_nonorth(anb_ctx* ctx, const double* rau, const double* gx, const double* gy, const double* gz,
+                      double* div_no);
+
 /* Solves the current pressure system A x = b with the configured preconditioned CG to
  * (p_tol, p_rel_tol); x holds the initial guess on entry.  *iters receives the count. */
 int anb_debug_pressure_solve(anb_ctx* ctx, const double* b, double* x, int* iters, double* final_res);

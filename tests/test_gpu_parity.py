@@ -70,6 +70,19 @@ def test_pressure_system(kw):
     assert np.abs(a["div_star"] - b["div_star"]).max() < 1e-12 * np.abs(b["phi_star"]).max()
 
 
+@pytest.mark.parametrize("kw", CASES)
+def test_nonorth_divergence(kw):
+    """k_nonorth_rhs alone: the divergence of the explicit non-orthogonal flux for a random rAU and
+    pressure-correction gradient, against the oracle's restatement of GSV1:1538-1593."""
+    m, bc, s, o = _pair(kw)
+    rng = np.random.default_rng(7)
+    rau = 1e-3 * (1 + 0.1 * rng.random(m.n_cells))
+    grad = rng.standard_normal((3, m.n_cells))
+    phi_no, div_ref = o.nonorth(rau, grad)
+    div = s.debug_nonorth(rau, grad)
+    assert np.abs(div - div_ref).max() <= 1e-12 * max(np.abs(phi_no).max(), 1e-300)
+
+
 @pytest.mark.parametrize("amg", [1, 0])
 def test_pressure_solve(amg):
     m, bc, s, o = _pair(dict(nx=40, ny=20, nz=20, jitter=0.15, seed=5), p_use_amg=amg, p_tol=1e-30,
