@@ -137,16 +137,19 @@ __global__ void k_bicg_loop_cond(cudaGraphConditionalHandle h, int* fl, int nc, 
   cudaGraphSetConditional(h, (!all_done(fl, nc) && t < maxTrips) ? 1u : 0u);
 }
 
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_bicg_init(BicgArgsT<T> a) {
   __shared__ double sm[6 * 32];
   const int n = a.A.n;
+  const bool all[3] = {true, true, true};
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    double ax[3];  // (A x)_r of every component, one pass over the row (same terms, same order)
+    row3<WM>(a.A, r, a.x, (size_t)n, all, a.nc, ax);
     _Pragma("unroll") for (int c = 0; c < 3; ++c) if (c < a.nc) {
       const size_t o = (size_t)c * n;
       const double bb = (double)a.b[o + r];
-      const double rr = bb - sell_row(a.A, r, a.x + o);
+      const double rr = bb - ax[c];
       a.r[o + r] = (T)rr;
       a.rh[o + r] = (T)rr;
       a.p[o + r] = T(0);
@@ -381,14 +384,17 @@ __global__ void __launch_bounds__(kBlock) k_bicg_x(BicgArgsT<T> a) {
 // ---------------------------------------------------------------- PCG
 // sc: 0 rz, 1 alpha, 2 beta, 3 eps, 4 rr, 5 pq ; fl: 0 done, 1 iters, 2 converged, 3 first
 
-template <class T>
+template <class T, int WM>
 __global__ void __launch_bounds__(kBlock) k_pcg_init(PcgArgsT<T> a) {
   __shared__ double sm[2 * 32];
   const int n = a.A.n;
+  const bool all[1] = {true};
   double acc[2] = {0, 0};
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const double bb = (double)a.b[r];
-    const double rr = bb - sell_row(a.A, r, a.x);
+    double ax[3];
+    row3<WM>(a.A, r, a.x, (size_t)n, all, 1, ax);  // the row in registers for WM > 0, same sum
+    const double rr = bb - ax[0];
     a.r[r] = (T)rr;
     acc[0] += rr * rr;
     acc[1] += bb * bb;
@@ -1037,7 +1043,7 @@ __global__ void __launch_bounds__(kBlock) k_apply_correction(size_t n, double* x
 template <class T>
 void bicg_init(const LaunchCfg& lc, const BicgArgsT<T>& a) {
   g_launches += 1;
-  k_bicg_init<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_bicg_init<T, W.value>, a); });
 }
 // One BiCGSTAB iteration; apply (when given) is the right preconditioner of the active
 // components after the p and the s updates (the vector kernels then leave ph and sh to it).
@@ -1081,7 +1087,7 @@ void bicg_iteration_precond(const LaunchCfg& lc, const BicgArgsT<T>& a, void (*a
 template <class T>
 void pcg_init(const LaunchCfg& lc, const PcgArgsT<T>& a) {
   g_launches += 1;
-  k_pcg_init<T><<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
+  with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_init<T, W.value>, a); });
 }
 
 static int blocks_for(int n, int cap) { return std::max(1, std::min(cap, (n + kBlock - 1) / kBlock)); }
