@@ -10,7 +10,8 @@ Workload (one "step" = one steady SIMPLE outer iteration of the reference's gene
   The mesh and fields are synthetic (generated here); device working set ~1.9 GB > 126 MB L2.
 
 Reference arm (--impl reference): the CPU oracle (oracle/, a C++/OpenMP restatement of the
-reference's SIMPLE iteration; the reference's own HYPRE path cannot be built without HYPRE and MPI)
+reference's SIMPLE iteration with an aggregation-AMG PCG for the pressure in place of HYPRE's
+BoomerAMG-PCG; the reference's own HYPRE path cannot be built without HYPRE and MPI)
 on the box's host cores, same case built by the oracle alone (no product library in the process),
 same warm-up and timed step indices as the library arm.
 
@@ -265,13 +266,14 @@ def ct_ll():
 
 
 def cpu_baseline(m, bc, state, steps: int = 1) -> dict:
-    """Oracle port (C++/OpenMP, Jacobi-PCG) on the same mesh: one SIMPLE step, all host threads."""
+    """Oracle port (C++/OpenMP, aggregation-AMG PCG for the pressure as the reference's BoomerAMG-PCG,
+    Jacobi-BiCGSTAB for the momentum) on the same mesh: one SIMPLE step, all host threads."""
     import oracle
 
     nthreads = os.cpu_count() or 1
     o = oracle.Oracle(m.topology())
     o.set_bc(bc)
-    prm = oracle.params(n_threads=nthreads, **PARAMS)
+    prm = oracle.params(n_threads=nthreads, p_use_amg=1, **PARAMS)
     t0 = time.perf_counter()
     o.run(prm, steps, *state)
     dt = time.perf_counter() - t0
@@ -290,7 +292,7 @@ def run_reference(args, rank: int, world: int) -> dict | None:
 
     o, bc, state = oracle.channel_case(**WORKLOAD)
     nthreads = os.cpu_count() or 1
-    prm = oracle.params(n_threads=nthreads, tol_mass=0.0, tol_vel=0.0, **PARAMS)  # no early stop
+    prm = oracle.params(n_threads=nthreads, tol_mass=0.0, tol_vel=0.0, p_use_amg=1, **PARAMS)  # no early stop
     s = {"u": state[0], "v": state[1], "w": state[2], "p": state[3]}
     if args.warmup > 0:
         s, _ = o.run(prm, args.warmup, *state)
@@ -308,7 +310,7 @@ def run_reference(args, rank: int, world: int) -> dict | None:
                          "sample": f"steps {args.warmup + 1}-{args.warmup + args.steps} of the workload (the "
                                    f"library arm's timed steps) after {args.warmup} warm-up steps; the "
                                    f"reference's HYPRE path cannot be built (no HYPRE/MPI), the oracle port "
-                                   f"(Jacobi-PCG / Jacobi-BiCGSTAB) stands in"},
+                                   f"(AMG-PCG / Jacobi-BiCGSTAB) stands in"},
         "e2e": {"value": v, "unit": "cell-iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -363,7 +365,7 @@ def run_variants(args) -> dict:
 
 
 def run_cpu_baselines(args) -> dict:
-    """The oracle port (C++/OpenMP, all host threads, Jacobi-PCG / Jacobi-BiCGSTAB at the reference's
+    """The oracle port (C++/OpenMP, all host threads, AMG-PCG / Jacobi-BiCGSTAB at the reference's
     1e-10 tolerances) on configurations 1-3, each case built by the oracle alone: config 1 (16,000
     hexes) for 300 steps from the initial state, config 2 (970,480 cells) and config 3 (3,977,792
     cells) on bounded samples of steps 1..k.  No product library is loaded."""
@@ -378,7 +380,7 @@ def run_cpu_baselines(args) -> dict:
         t0 = time.perf_counter()
         o, bc, state = oracle.channel_case(**kw)
         setup = time.perf_counter() - t0
-        prm = oracle.params(n_threads=nthreads, tol_mass=0.0, tol_vel=0.0, **PARAMS)
+        prm = oracle.params(n_threads=nthreads, tol_mass=0.0, tol_vel=0.0, p_use_amg=1, **PARAMS)
         t0 = time.perf_counter()
         _, st = o.run(prm, steps, *state)
         dt = time.perf_counter() - t0

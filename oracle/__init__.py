@@ -25,7 +25,7 @@ class OrcParams(ct.Structure):
                 ("vel_maxit", ct.c_int), ("vel_tol", ct.c_double), ("vel_rel_tol", ct.c_double),
                 ("p_maxit", ct.c_int), ("p_tol", ct.c_double), ("p_rel_tol", ct.c_double),
                 ("corr_tol", ct.c_double), ("tol_mass", ct.c_double), ("tol_vel", ct.c_double),
-                ("n_threads", ct.c_int)]
+                ("n_threads", ct.c_int), ("p_use_amg", ct.c_int)]
 
 
 class OrcStats(ct.Structure):
@@ -267,7 +267,7 @@ def params(**kw) -> OrcParams:
     """Oracle controls with the reference defaults (main.cu:73-103)."""
     p = OrcParams(rho=1.0, mu=0.05, u_relax=0.7, p_relax=1.0, n_nonorth_corr=2, n_vel_nonorth_corr=0,
                   n_pressure_corr=0, vel_maxit=100, vel_tol=1e-10, vel_rel_tol=0.0, p_maxit=4000, p_tol=1e-10,
-                  p_rel_tol=0.0, corr_tol=1e-12, tol_mass=1e-10, tol_vel=1e-10, n_threads=0)
+                  p_rel_tol=0.0, corr_tol=1e-12, tol_mass=1e-10, tol_vel=1e-10, n_threads=0, p_use_amg=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -613,9 +613,204 @@ int bicgstab(const CSR& A, const std::vector<double>& vals, const std::vector<do
   return it;
 }
 
-// Jacobi-preconditioned CG; stop when ||r||_2 <= max(atol, rtol*||b||).
+// ---- aggregation AMG for the CPU pressure solve (stand-in for the reference's BoomerAMG, ----
+// GSV1:2242-2260; an implementation of its own, not the B200 library's).  Rebuilt from every outer
+// step's pressure matrix, as the reference rebuilds its hierarchy at pAmgRebuildEvery = 1
+// (GSV1:3409-3411): greedy aggregation on strong negative couplings (-a_ij >= 0.25 max_k -a_ik; a
+// row and its free strong neighbours form an aggregate, leftover rows join their strongest
+// neighbour's), piecewise-constant prolongation, Galerkin coarse operators down to <= 200 rows,
+// Cholesky there; a symmetric V(1,1) cycle with weighted Jacobi (0.9) and the coarse correction
+// scaled by 1.6 (over-correction keeps it SPD).  Used by the timed CPU baseline (p_use_amg).
+struct AmgLev {
+  int n = 0, nc = 0;
+  std::vector<int> off, col;     // CSR, diagonal included
+  std::vector<double> val, diag;
+  std::vector<int> agg, memOff, mem;
+  std::vector<double> b, x, r;
+};
+struct CpuAmg {
+  std::vector<AmgLev> lv;
+  std::vector<double> L;  // Cholesky factor of the coarsest level (row-major, lower)
+  std::vector<char> skip;
+};
+
+void amg_build(const CSR& A, const std::vector<double>& vals, CpuAmg& H) {
+  H.lv.clear();
+  AmgLev l0;
+  l0.n = A.n;
+  l0.off = A.rowOff;
+  l0.col = A.cols;
+  l0.val = vals;
+  H.lv.push_back(std::move(l0));
+  for (;;) {
+    AmgLev& f = H.lv.back();
+    const int n = f.n;
+    f.diag.assign(n, 0.0);
+    for (int i = 0; i < n; ++i)
+      for (int k = f.off[i]; k < f.off[i + 1]; ++k)
+        if (f.col[k] == i) f.diag[i] = f.val[k];
+    f.b.assign(n, 0.0);
+    f.x.assign(n, 0.0);
+    f.r.assign(n, 0.0);
+    if (n <= 200 || H.lv.size() >= 20) break;
+    std::vector<double> mx(n, 0.0);
+    for (int i = 0; i < n; ++i)
+      for (int k = f.off[i]; k < f.off[i + 1]; ++k)
+        if (f.col[k] != i) mx[i] = std::max(mx[i], -f.val[k]);
+    auto strong = [&](int i, int k) { return f.col[k] != i && -f.val[k] > 0.0 && -f.val[k] >= 0.25 * mx[i]; };
+    f.agg.assign(n, -1);
+    int nc = 0;
+    for (int i = 0; i < n; ++i) {
+      if (f.agg[i] >= 0) continue;
+      bool free = true;
+      for (int k = f.off[i]; k < f.off[i + 1] && free; ++k)
+        if (strong(i, k) && f.agg[f.col[k]] >= 0) free = false;
+      if (!free) continue;
+      f.agg[i] = nc;
+      for (int k = f.off[i]; k < f.off[i + 1]; ++k)
+        if (strong(i, k)) f.agg[f.col[k]] = nc;
+      ++nc;
+    }
+    std::vector<int> first(f.agg);
+    for (int i = 0; i < n; ++i) {
+      if (first[i] >= 0) continue;
+      int best = -1;
+      double bv = 0.0;
+      for (int k = f.off[i]; k < f.off[i + 1]; ++k)
+        if (strong(i, k) && first[f.col[k]] >= 0 && -f.val[k] > bv) {
+          bv = -f.val[k];
+          best = first[f.col[k]];
+        }
+      f.agg[i] = best >= 0 ? best : nc++;
+    }
+    if (nc > 0.9 * n) break;  // coarsening stalled: this level is the coarsest
+    f.nc = nc;
+    f.memOff.assign(nc + 1, 0);
+    for (int i = 0; i < n; ++i) f.memOff[f.agg[i] + 1]++;
+    for (int I = 0; I < nc; ++I) f.memOff[I + 1] += f.memOff[I];
+    f.mem.assign(n, 0);
+    {
+      std::vector<int> fill(f.memOff.begin(), f.memOff.end() - 1);
+      for (int i = 0; i < n; ++i) f.mem[fill[f.agg[i]]++] = i;
+    }
+    AmgLev c;
+    c.n = nc;
+    c.off.assign(nc + 1, 0);
+    std::vector<int> mark(nc, -1), pos(nc, 0);
+    for (int I = 0; I < nc; ++I) {
+      const size_t start = c.col.size();
+      for (int m = f.memOff[I]; m < f.memOff[I + 1]; ++m) {
+        const int i = f.mem[m];
+        for (int k = f.off[i]; k < f.off[i + 1]; ++k) {
+          const int J = f.agg[f.col[k]];
+          if (mark[J] != I) {
+            mark[J] = I;
+            pos[J] = (int)c.col.size();
+            c.col.push_back(J);
+            c.val.push_back(0.0);
+          }
+          c.val[pos[J]] += f.val[k];
+        }
+      }
+      c.off[I + 1] = (int)c.col.size();
+      (void)start;
+    }
+    H.lv.push_back(std::move(c));
+  }
+  // Cholesky of the coarsest level; a pivot below 1e-13 of the largest diagonal (a singular,
+  // all-Neumann system) drops its row and column
+  const AmgLev& d = H.lv.back();
+  const int nd = d.n;
+  std::vector<double> M((size_t)nd * nd, 0.0);
+  double dm = 0.0;
+  for (int i = 0; i < nd; ++i) {
+    for (int k = d.off[i]; k < d.off[i + 1]; ++k) M[(size_t)i * nd + d.col[k]] += d.val[k];
+    dm = std::max(dm, std::fabs(d.diag[i]));
+  }
+  H.L.assign((size_t)nd * nd, 0.0);
+  H.skip.assign(nd, 0);
+  for (int j = 0; j < nd; ++j) {
+    double s = M[(size_t)j * nd + j];
+    for (int k = 0; k < j; ++k) s -= H.L[(size_t)j * nd + k] * H.L[(size_t)j * nd + k];
+    if (s <= 1e-13 * dm) {
+      H.skip[j] = 1;
+      continue;
+    }
+    const double ljj = std::sqrt(s);
+    H.L[(size_t)j * nd + j] = ljj;
+    for (int i = j + 1; i < nd; ++i) {
+      double t = M[(size_t)i * nd + j];
+      for (int k = 0; k < j; ++k) t -= H.L[(size_t)i * nd + k] * H.L[(size_t)j * nd + k];
+      H.L[(size_t)i * nd + j] = t / ljj;
+    }
+  }
+}
+
+void amg_vcycle(CpuAmg& H, size_t l) {
+  AmgLev& f = H.lv[l];
+  const int n = f.n;
+  if (l + 1 == H.lv.size()) {  // coarsest: L L^T x = b
+    std::vector<double>& y = f.x;
+    for (int i = 0; i < n; ++i) {
+      if (H.skip[i]) { y[i] = 0.0; continue; }
+      double s = f.b[i];
+      for (int k = 0; k < i; ++k) s -= H.L[(size_t)i * n + k] * y[k];
+      y[i] = s / H.L[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      if (H.skip[i]) { y[i] = 0.0; continue; }
+      double s = y[i];
+      for (int k = i + 1; k < n; ++k) s -= H.L[(size_t)k * n + i] * y[k];
+      y[i] = s / H.L[(size_t)i * n + i];
+    }
+    return;
+  }
+  const double w = 0.9, corr = 1.6;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) f.x[i] = w * f.b[i] / f.diag[i];
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int k = f.off[i]; k < f.off[i + 1]; ++k) s += f.val[k] * f.x[f.col[k]];
+    f.r[i] = f.b[i] - s;
+  }
+  AmgLev& c = H.lv[l + 1];
+#pragma omp parallel for schedule(static)
+  for (int I = 0; I < f.nc; ++I) {
+    double s = 0.0;
+    for (int m = f.memOff[I]; m < f.memOff[I + 1]; ++m) s += f.r[f.mem[m]];
+    c.b[I] = s;
+  }
+  amg_vcycle(H, l + 1);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) f.x[i] += corr * c.x[f.agg[i]];
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int k = f.off[i]; k < f.off[i + 1]; ++k) s += f.val[k] * f.x[f.col[k]];
+    f.r[i] = f.b[i] - s;
+  }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) f.x[i] += w * f.r[i] / f.diag[i];
+}
+
+// z = M^-1 r: Jacobi, or one V-cycle of the hierarchy when given
+void precondition(CpuAmg* amg, const std::vector<double>& dinv, const std::vector<double>& r, std::vector<double>& z) {
+  const int n = (int)r.size();
+  if (!amg) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
+    return;
+  }
+  AmgLev& f = amg->lv[0];
+  std::copy(r.begin(), r.end(), f.b.begin());
+  amg_vcycle(*amg, 0);
+  std::copy(f.x.begin(), f.x.end(), z.begin());
+}
+
+// Preconditioned CG (Jacobi, or the AMG V-cycle above); stop when ||r||_2 <= max(atol, rtol*||b||).
 int pcg(const CSR& A, const std::vector<double>& vals, const std::vector<double>& b, std::vector<double>& x,
-        double atol, double rtol, int maxit, bool* conv) {
+        double atol, double rtol, int maxit, bool* conv, CpuAmg* amg = nullptr) {
   const int n = A.n;
   std::vector<double> dinv(n), r(n), z(n), p(n), q(n);
   for (int i = 0; i < n; ++i) {
@@ -629,7 +824,8 @@ int pcg(const CSR& A, const std::vector<double>& vals, const std::vector<double>
   double rr = det_sum(n, [&](int i) { return r[i] * r[i]; });
   *conv = true;
   if (std::sqrt(rr) <= eps) return 0;
-  for (int i = 0; i < n; ++i) { z[i] = dinv[i] * r[i]; p[i] = z[i]; }
+  precondition(amg, dinv, r, z);
+  for (int i = 0; i < n; ++i) p[i] = z[i];
   double rz = det_sum(n, [&](int i) { return r[i] * z[i]; });
   int it = 0;
   while (it < maxit) {
@@ -640,8 +836,7 @@ int pcg(const CSR& A, const std::vector<double>& vals, const std::vector<double>
     for (int i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; }
     rr = det_sum(n, [&](int i) { return r[i] * r[i]; });
     if (std::sqrt(rr) <= eps) return it;
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < n; ++i) z[i] = dinv[i] * r[i];
+    precondition(amg, dinv, r, z);
     double rzN = det_sum(n, [&](int i) { return r[i] * z[i]; });
     double beta = rzN / rz;
     rz = rzN;
@@ -857,6 +1052,7 @@ int orc_simple_run(orc_mesh* mp, const orc_params* prm, int nsteps, double* uIO,
   std::vector<double> uOld(n), vOld(n), wOld(n), pOld(n), uS(n), vS(n), wS(n), pCorr(n), rAU(n), rhs(n);
   std::vector<double> phiStar(m.nFaces), phi(m.nFaces), phiNO(m.nFaces), divStar(n), divCorr(n), divNO(n);
   std::vector<double> pvals(m.pat.vals.size());
+  CpuAmg amg;  // pressure preconditioner with p_use_amg, rebuilt every outer step
   int done = 0;
   for (int step = 1; step <= nsteps; ++step) {
     uOld = u; vOld = v; wOld = w; pOld = p;
@@ -892,6 +1088,7 @@ int orc_simple_run(orc_mesh* mp, const orc_params* prm, int nsteps, double* uIO,
       *qs[comp] = qIter;
     }
     pressure_matrix(m, rAU.data(), pvals);  // GSV1:3407-3411
+    if (prm->p_use_amg) amg_build(m.pat, pvals, amg);
     u = uS; v = vS; w = wS; p = pOld;
     lsq_grad(m, 3, p.data(), gp.x.data(), gp.y.data(), gp.z.data());
     rhie_chow(m, prm->rho, u.data(), v.data(), w.data(), p.data(), gp, rAU.data(), phiStar);
@@ -911,7 +1108,7 @@ int orc_simple_run(orc_mesh* mp, const orc_params* prm, int nsteps, double* uIO,
       ++counter;
       double rtol = (counter == total) ? 0.0 : prm->p_rel_tol;
       bool conv = true;
-      pLast = pcg(m.pat, pvals, b, pCorr, prm->p_tol, rtol, prm->p_maxit, &conv);
+      pLast = pcg(m.pat, pvals, b, pCorr, prm->p_tol, rtol, prm->p_maxit, &conv, prm->p_use_amg ? &amg : nullptr);
       anyNC = anyNC || !conv;
       pTot += pLast;
       if (pc == nPS) {
@@ -927,7 +1124,7 @@ int orc_simple_run(orc_mesh* mp, const orc_params* prm, int nsteps, double* uIO,
       ++counter;
       double rtol = (counter == total) ? 0.0 : prm->p_rel_tol;
       bool conv = true;
-      pLast = pcg(m.pat, pvals, b, dpc, prm->p_tol, rtol, prm->p_maxit, &conv);
+      pLast = pcg(m.pat, pvals, b, dpc, prm->p_tol, rtol, prm->p_maxit, &conv, prm->p_use_amg ? &amg : nullptr);
       anyNC = anyNC || !conv;
       pTot += pLast;
       for (int c = 0; c < n; ++c) pCorr[c] += 1.0 * dpc[c];

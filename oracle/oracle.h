@@ -29,6 +29,7 @@ typedef struct orc_params {
   int p_maxit; double p_tol, p_rel_tol;
   double corr_tol, tol_mass, tol_vel;
   int n_threads;
+  int p_use_amg;  /* 1: pressure PCG preconditioned by the oracle's aggregation AMG, else Jacobi */
 } orc_params;
 
 typedef struct orc_stats {
