@@ -449,17 +449,13 @@ void fill_info(anb_adjoint_info* info, const KrylovResult& kr, double secs, cons
 
 void upload4(anb_ctx* c, const double* src, double* dst) {
   const size_t C = c->C;
-  const double* s3[3] = {src, src + C, src + 2 * C};
-  upload_cells(c, s3, dst, 3);
-  const double* s1[1] = {src + 3 * C};
-  upload_cells(c, s1, dst + 3 * C, 1);
+  const double* s4[4] = {src, src + C, src + 2 * C, src + 3 * C};
+  upload_cells(c, s4, dst, 4);
 }
 void download4(anb_ctx* c, const double* src, double* dst) {
   const size_t C = c->C;
-  double* d3[3] = {dst, dst + C, dst + 2 * C};
-  download_cells(c, src, d3, 3);
-  double* d1[1] = {dst + 3 * C};
-  download_cells(c, src + 3 * C, d1, 1);
+  double* d4[4] = {dst, dst + C, dst + 2 * C, dst + 3 * C};
+  download_cells(c, src, d4, 4);
 }
 // Dirichlet-value arrays: 3 x nFaces (input order) <-> 3 x nBoundary (device)
 void upload_bc3(anb_ctx* c, const double* src, double* dst) {

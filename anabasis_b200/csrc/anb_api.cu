@@ -30,35 +30,88 @@ void permute_in(const anb_ctx* c, const double* src, std::vector<double>& dst, i
     for (int r = 0; r < c->C; ++r) dst[(size_t)q * c->C + r] = src[(size_t)q * c->C + c->L.new2old[r]];
 }
 
-// Cell fields cross the host/device boundary through a pinned staging buffer (3 * nCells):
-// the host permutes into / out of it, the copy engine moves it with one DMA.
-void upload_cells(anb_ctx* c, const double* const* src, double* dst, int comps) {
-  double* h = c->hStage;
-  const int* n2o = c->L.new2old.data();
-  const int C = c->C;
-  for (int q = 0; q < comps; ++q) {
-    const double* s = src[q];
-    double* d = h + (size_t)q * C;
-#pragma omp parallel for schedule(static) if (C > 200000)
-    for (int r = 0; r < C; ++r) d[r] = s[n2o[r]];
+// Cell fields cross the host/device boundary in input numbering.  Upload: the host copies the
+// caller's arrays into the pinned staging buffer chunk by chunk, each chunk's DMA running while the
+// next one is copied, and one kernel gathers the staged fields into layout numbering.  Download: the
+// kernel gathers into input numbering, the DMAs go out chunk by chunk and each chunk is copied to
+// the caller's array as soon as its event has completed.  No permutation runs on the host.
+size_t stage_chunk(size_t C) { return std::max<size_t>((size_t)1 << 18, (C + 15) / 16); }
+
+void host_copy(double* d, const double* s, size_t n) {
+  constexpr size_t kB = 8192;
+  const ptrdiff_t nb = (ptrdiff_t)((n + kB - 1) / kB);
+#pragma omp parallel for schedule(static) if (nb > 8)
+  for (ptrdiff_t b = 0; b < nb; ++b) {
+    const size_t o = (size_t)b * kB;
+    std::memcpy(d + o, s + o, sizeof(double) * std::min(kB, n - o));
   }
-  CK(cudaMemcpyAsync(dst, h, (size_t)comps * C * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+}
+
+void upload_cells(anb_ctx* c, const double* const* src, double* const* dst, int comps) {
+  if (comps < 1 || comps > 4) throw AnbError(ANB_ERR_INVALID, "upload of more than 4 cell fields");
+  const size_t C = c->C, ch = stage_chunk(C);
+  PermuteArgs a{};
+  a.idx = c->dN2O;
+  a.n = c->C;
+  a.comps = comps;
+  for (int q = 0; q < comps; ++q) {
+    double* h = c->hStage + q * C;
+    double* d = c->dStage + q * C;
+    for (size_t o = 0; o < C; o += ch) {
+      const size_t n = std::min(ch, C - o);
+      host_copy(h + o, src[q] + o, n);
+      CK(cudaMemcpyAsync(d + o, h + o, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    a.src[q] = d;
+    a.dst[q] = dst[q];
+  }
+  launch_permute_cells(c->lc, a);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->stream));
 }
 
-void download_cells(anb_ctx* c, const double* src, double* const* dst, int comps) {
-  double* h = c->hStage;
-  const int* n2o = c->L.new2old.data();
-  const int C = c->C;
-  CK(cudaMemcpyAsync(h, src, (size_t)comps * C * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+void upload_cells(anb_ctx* c, const double* const* src, double* dst, int comps) {
+  double* d[4] = {};
+  for (int q = 0; q < comps && q < 4; ++q) d[q] = dst + (size_t)q * c->C;
+  upload_cells(c, src, d, comps);
+}
+
+void download_cells(anb_ctx* c, const double* const* src, double* const* dst, int comps) {
+  if (comps < 1 || comps > 4) throw AnbError(ANB_ERR_INVALID, "download of more than 4 cell fields");
+  const size_t C = c->C, ch = stage_chunk(C);
+  PermuteArgs a{};
+  a.idx = c->dO2N;
+  a.n = c->C;
+  double* out[4] = {};
   for (int q = 0; q < comps; ++q) {
-    double* d = dst[q];
-    if (!d) continue;
-    const double* s = h + (size_t)q * C;
-#pragma omp parallel for schedule(static) if (C > 200000)
-    for (int r = 0; r < C; ++r) d[n2o[r]] = s[r];
+    if (!dst[q]) continue;
+    a.src[a.comps] = src[q];
+    a.dst[a.comps] = c->dStage + a.comps * C;
+    out[a.comps++] = dst[q];
   }
+  if (a.comps == 0) return;
+  launch_permute_cells(c->lc, a);
+  CK(cudaGetLastError());
+  int ev = 0;
+  for (int k = 0; k < a.comps; ++k)
+    for (size_t o = 0; o < C; o += ch) {
+      const size_t n = std::min(ch, C - o);
+      CK(cudaMemcpyAsync(c->hStage + k * C + o, c->dStage + k * C + o, n * sizeof(double),
+                         cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaEventRecord(c->stageEv[ev++], c->stream));
+    }
+  ev = 0;
+  for (int k = 0; k < a.comps; ++k)
+    for (size_t o = 0; o < C; o += ch) {
+      CK(cudaEventSynchronize(c->stageEv[ev++]));
+      host_copy(out[k] + o, c->hStage + k * C + o, std::min(ch, C - o));
+    }
+}
+
+void download_cells(anb_ctx* c, const double* src, double* const* dst, int comps) {
+  const double* s[4] = {};
+  for (int q = 0; q < comps && q < 4; ++q) s[q] = src + (size_t)q * c->C;
+  download_cells(c, s, dst, comps);
 }
 
 // Face array on the device (new order, new orientation) -> input order and orientation.
@@ -1063,6 +1116,9 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     dm.fNeigh = A.upload(L.fNeigh);
     dm.face = c->dFace;
     dm.fFlags = A.upload(L.fFlags);
+    c->dN2O = A.upload(L.new2old);
+    c->dO2N = A.upload(L.old2new);
+    c->dStage = A.alloc<double>((size_t)4 * c->C);
     {
       const size_t nE = (size_t)c->nEnt;
       dm.nEnt = c->nEnt;
@@ -1182,7 +1238,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     CK(cudaMemset(c->Pc, 0, sizeof(double) * C));
     CK(cudaMallocHost(&c->hFlags, sizeof(int) * kFlagCount));
     CK(cudaMallocHost(&c->hScal, sizeof(double) * 64));
-    CK(cudaMallocHost(&c->hStage, sizeof(double) * 3 * C));
+    CK(cudaMallocHost(&c->hStage, sizeof(double) * 4 * C));
+    for (auto& e : c->stageEv) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CK(cudaMallocHost(&c->hDefer, sizeof(int) * kDeferSlots * kDeferInts));
     CK(cudaDeviceSynchronize());
     lap(3);
@@ -1196,6 +1253,8 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
     if (c->hScal) cudaFreeHost(c->hScal);
     if (c->hStage) cudaFreeHost(c->hStage);
     if (c->hDefer) cudaFreeHost(c->hDefer);
+    for (auto e : c->stageEv)
+      if (e) cudaEventDestroy(e);
     return rc;
   }
   *out = c.release();
@@ -1220,6 +1279,8 @@ void anb_destroy(anb_ctx* c) {
   if (c->hScal) cudaFreeHost(c->hScal);
   if (c->hStage) cudaFreeHost(c->hStage);
   if (c->hDefer) cudaFreeHost(c->hDefer);
+  for (auto e : c->stageEv)
+    if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1284,11 +1345,10 @@ int anb_set_state(anb_ctx* c, const double* u, const double* v, const double* w,
   return guarded(c, [&]() -> int {
     if (!u || !v || !w || !p) throw AnbError(ANB_ERR_INVALID, "null state array");
     CK(cudaSetDevice(c->prm.device));
-    const double* s3[3] = {u, v, w};
-    upload_cells(c, s3, c->U, 3);
-    const double* s1[1] = {p};
-    upload_cells(c, s1, c->P, 1);
-    CK(cudaMemset(c->phi, 0, sizeof(double) * ((size_t)c->nI + c->nB)));
+    const double* s4[4] = {u, v, w, p};
+    double* d4[4] = {c->U, c->U + c->C, c->U + 2 * (size_t)c->C, c->P};
+    CK(cudaMemsetAsync(c->phi, 0, sizeof(double) * ((size_t)c->nI + c->nB), c->stream));
+    upload_cells(c, s4, d4, 4);
     c->stateSet = true;
     return ANB_OK;
   });
@@ -1298,10 +1358,9 @@ int anb_get_state(anb_ctx* c, double* u, double* v, double* w, double* p, double
   if (!c) return ANB_ERR_INVALID;
   return guarded(c, [&]() -> int {
     CK(cudaSetDevice(c->prm.device));
-    double* d3[3] = {u, v, w};
-    download_cells(c, c->U, d3, 3);
-    double* d1[1] = {p};
-    if (p) download_cells(c, c->P, d1, 1);
+    const double* s4[4] = {c->U, c->U + c->C, c->U + 2 * (size_t)c->C, c->P};
+    double* d4[4] = {u, v, w, p};
+    download_cells(c, s4, d4, 4);
     if (phi) download_faces(c, c->phi, phi);
     return ANB_OK;
   });

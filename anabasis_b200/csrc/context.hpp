@@ -111,7 +111,14 @@ struct anb_ctx {
   int* hDefer = nullptr;
   int nDefer = 0;
   double* hScal = nullptr;
-  double* hStage = nullptr;   // 3 * nCells staging for cell fields
+  // cell fields cross the host/device boundary through 4 * nCells pinned doubles (hStage) and
+  // 4 * nCells device doubles in input numbering (dStage), permuted on the device by the new->old
+  // (dN2O) and old->new (dO2N) cell maps; stageEv marks the chunks of a download
+  static constexpr int kStageEvents = 64;
+  double* hStage = nullptr;
+  double* dStage = nullptr;
+  int *dN2O = nullptr, *dO2N = nullptr;
+  cudaEvent_t stageEv[kStageEvents] = {};
   // state
   bool bcSet = false, stateSet = false, pZeroBC = true;
   long long outerStep = 0;
@@ -182,7 +189,11 @@ int guarded(anb_ctx* c, F&& f) {
   }
 }
 
+// comps <= 4 cell fields in input numbering <-> device arrays in layout numbering; the
+// single-pointer forms take comps consecutive nCells blocks on the device
+void upload_cells(anb_ctx* c, const double* const* src, double* const* dst, int comps);
 void upload_cells(anb_ctx* c, const double* const* src, double* dst, int comps);
+void download_cells(anb_ctx* c, const double* const* src, double* const* dst, int comps);
 void download_cells(anb_ctx* c, const double* src, double* const* dst, int comps);
 DSell mom_sell(const anb_ctx* c);
 DSell p_sell(const anb_ctx* c);

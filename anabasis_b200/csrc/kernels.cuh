@@ -228,6 +228,14 @@ void launch_flux_final(const LaunchCfg& lc, const DMesh& m, const FluxArgs& a);
 // Extra pressure passes: b = -divCorr and dx = 0; y += s x.
 void launch_pass_rhs(const LaunchCfg& lc, int n, const double* divCorr, double* b, double* dx);
 void launch_add_scaled(const LaunchCfg& lc, int n, double s, const double* x, double* y);
+// Cell fields between input and layout numbering: dst[q][i] = src[q][idx[i]], q < comps <= 4
+struct PermuteArgs {
+  const int* idx;
+  const double* src[4];
+  double* dst[4];
+  int n, comps;
+};
+void launch_permute_cells(const LaunchCfg& lc, const PermuteArgs& a);
 // out[2q], out[2q+1] = sum (after_q - before_q)^2, sum after_q^2 over n rows, q = 0..2 (device)
 void launch_relchg3(const LaunchCfg& lc, int n, const double* before, const double* after, Reducer red,
                     double* out);

@@ -656,6 +656,21 @@ __global__ void __launch_bounds__(kBlock) k_add_scaled(int n, double s, const do
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] += s * x[i];
 }
 
+// Cell-field permutation for the host/device boundary (input <-> layout numbering).  The index is
+// read once per row and every component's gather issued before its store.
+__global__ void __launch_bounds__(kBlock) k_permute_cells(PermuteArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const int j = a.idx[i];
+    double v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (q < a.comps) v[q] = a.src[q][j];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (q < a.comps) a.dst[q][i] = v[q];
+  }
+}
+
 // Relative change of the three momentum iterates (main.cu:3377-3379): per component the sum of
 // (after - before)^2 and of after^2, combined in block order into out[0..5].
 __global__ void __launch_bounds__(kBlock) k_relchg3(int n, const double* before, const double* after, Reducer red,
@@ -680,6 +695,10 @@ __global__ void __launch_bounds__(kBlock) k_relchg3(int n, const double* before,
 void launch_pass_rhs(const LaunchCfg& lc, int n, const double* divCorr, double* b, double* dx) {
   g_launches += 1;
   k_pass_rhs<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(n, divCorr, b, dx);
+}
+void launch_permute_cells(const LaunchCfg& lc, const PermuteArgs& a) {
+  g_launches += 1;
+  k_permute_cells<<<lc.rowBlocks, kBlock, 0, lc.stream>>>(a);
 }
 void launch_add_scaled(const LaunchCfg& lc, int n, double s, const double* x, double* y) {
   g_launches += 1;
