@@ -187,11 +187,6 @@ int defer_flags(anb_ctx* c, const int* dflags, int count) {
   return slot;
 }
 
-// PCG flag 5: a staged SpMV block whose shared-memory stage did not arrive within its poll limit.
-void check_stage_flag(const int* f) {
-  if (f[5]) throw AnbError(ANB_ERR_CUDA, "PCG: a bulk-copy stage of the staged SpMV did not arrive in time");
-}
-
 // Fills a solve's iterations and convergence from its flags (hDefer slot, after the stream has
 // synchronised, or hFlags right after a poll) and books the kernels its loop graph ran: one
 // condition kernel per evaluation, two iterations per body run.
@@ -208,7 +203,6 @@ void resolve_solve(anb_ctx* c, SolveOut& o) {
     }
     c->lastMomIts = std::max(1, mx);
   } else {
-    check_stage_flag(f);
     o.its[0] = f[1];
     o.conv[0] = f[2] != 0;
     c->lastPIts = std::max(1, o.its[0]);
@@ -355,11 +349,10 @@ int pcg_iterate(anb_ctx* c, const PcgArgsT<T>& a, const AmgDevT<T>* amg, SolveOu
   if (amg && !timed && pcg_loop_launch(c->lc, a, *amg)) {
     if (out) {
       out->kernelsPerIteration = 1 + amg->graphKernels;
-      out->slot = defer_flags(c, a.fl, 6);
+      out->slot = defer_flags(c, a.fl, 5);
       return 0;
     }
-    poll(c, a.fl, 6);
-    check_stage_flag(c->hFlags);
+    poll(c, a.fl, 5);
     const int trips = c->hFlags[4];
     g_launches += trips + 2LL * std::max(trips - 1, 0) * (1 + amg->graphKernels);
     return 0;
@@ -369,8 +362,7 @@ int pcg_iterate(anb_ctx* c, const PcgArgsT<T>& a, const AmgDevT<T>* amg, SolveOu
   const int tail = std::max(2, c->lastPIts / 8);
   while (true) {
     for (int k = 0; k < batch; ++k) pcg_iteration(c->lc, a, it++, amg);
-    poll(c, a.fl, 6);
-    check_stage_flag(c->hFlags);
+    poll(c, a.fl, 4);
     if (c->hFlags[0] || it > a.maxit + 2) break;
     batch = tail;
   }

@@ -166,7 +166,7 @@ namespace anb {
 constexpr int kScalBicg = 0;    // 3 * 8
 constexpr int kScalPcg = 24;    // 8
 constexpr int kFlagBicg = 0;    // 3 * 4
-constexpr int kFlagPcg = 32;    // 8: done, iterations, converged, first, loop-graph trips, stage timeout
+constexpr int kFlagPcg = 32;    // 8: done, iterations, converged, first, loop-graph trips
 constexpr int kFlagCount = 40;  // ints in anb_ctx::flags (and hFlags)
 constexpr int kDeferSlots = 64;
 constexpr int kDeferInts = 16;

@@ -122,48 +122,6 @@ inline int launch_width_class(int maxW) {
   return wc;
 }
 
-// ---- bulk copies (TMA, non-tensor) from global to this CTA's shared memory ----------------
-// One thread arms an mbarrier with the byte count (arrive.expect_tx) and issues the copies, each
-// completing its bytes on that barrier; the readers wait on the barrier's phase parity.  Source
-// and destination 16-byte aligned, sizes multiples of 16 bytes.  No multicast.
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-// makes initialised barriers visible to the async (TMA) proxy; a __syncthreads follows
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase of the given parity: false after `limit` polls (each poll may
-// suspend the thread for a hardware-defined interval), so no wait can hang the kernel.
-constexpr int kMbarPollLimit = 1 << 16;
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (int i = 0; i < kMbarPollLimit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
 // Cross-block deterministic reductions: each block writes a partial, the last block to arrive
 // (atomic ticket) combines the partials in block order.
 struct Reducer {

@@ -57,17 +57,7 @@ struct LaunchCfg {
 
 // Blocks of kBlock threads of `kernel` that fit on one SM at once (registers, shared memory);
 // queried once per kernel.
-int resident_blocks(const void* kernel, size_t dynSmem = 0);
-
-// SELL matrices whose slots may be staged in shared memory by bulk copies: value and column
-// arrays 16-byte aligned (every slice offset is a multiple of 32 slots).  ANB_SELL_STAGED=0
-// keeps the register kernels everywhere, for measurements.
-template <class T>
-inline bool sell_staged(const DSellT<T>& A) {
-  const char* s = std::getenv("ANB_SELL_STAGED");  // read per launch: graphs keep what they captured
-  return !(s && s[0] == '0') && A.sliceOff && (reinterpret_cast<uintptr_t>(A.val) & 15u) == 0 &&
-         (reinterpret_cast<uintptr_t>(A.col) & 15u) == 0;
-}
+int resident_blocks(const void* kernel);
 
 // Grid of a grid-stride row kernel: one full wave of its resident blocks on every SM, at most
 // `cap`.  With more blocks than fit, the blocks past the first wave run on a partly idle GPU at the
@@ -308,7 +298,7 @@ struct PcgArgsT {
   int mode;           // 0: PCG iteration; 1: plain preconditioner application z = M^-1 r (no update of
                       // x or r, no r.z reduction; fl[0] is the caller's done flag)
   double* sc;         // rz, alpha, beta, eps, rr, pq
-  int* fl;            // done, iters, converged, first, loop-graph trips (pcg_capture_loop), stage timeout
+  int* fl;            // done, iters, converged, first, loop-graph trips (pcg_capture_loop)
   double atol, rtol;
   int maxit;
   Reducer red;

@@ -712,14 +712,14 @@ void launch_relchg3(const LaunchCfg& lc, int n, const double* before, const doub
 
 std::atomic<long long> g_launches{0};
 
-int resident_blocks(const void* kernel, size_t dynSmem) {
+int resident_blocks(const void* kernel) {
   static std::mutex mu;
-  static std::unordered_map<const void*, int> cache;  // one dynamic shared size per kernel
+  static std::unordered_map<const void*, int> cache;
   std::lock_guard<std::mutex> lock(mu);
   auto it = cache.find(kernel);
   if (it != cache.end()) return it->second;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBlock, dynSmem) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBlock, 0) != cudaSuccess) {
     cudaGetLastError();
     n = 0;  // unknown: the caller keeps its cap
   }

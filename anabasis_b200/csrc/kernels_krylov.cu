@@ -408,7 +408,6 @@ __global__ void __launch_bounds__(kBlock) k_pcg_init(PcgArgsT<T> a) {
     a.fl[2] = a.fl[0];
     a.fl[3] = 1;
     a.fl[4] = 0;
-    a.fl[5] = 0;
   }
 }
 
@@ -464,102 +463,6 @@ __global__ void __launch_bounds__(kBlock) k_pcg_pq(PcgArgsT<T> a, const T* pOld,
     pNew[r] = (T)pr;
     a.q[r] = (T)q;
     acc[0] += pr * q;
-  }
-  if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
-    a.sc[5] = acc[0];
-    a.sc[1] = acc[0] != 0.0 ? a.sc[0] / acc[0] : 0.0;
-    a.fl[3] = 0;
-  }
-}
-
-// k_pcg_pq with the matrix slots staged in shared memory by bulk copies, one pipeline per warp.
-// A warp works on SELL-32 slices (32 rows, whose values and columns are contiguous) in the same
-// grid-stride order as k_pcg_pq; its lane 0 copies the warp's next slice into the other of two
-// stages while the warp computes the current one, so the only dependent global loads left per row
-// are the gathers of z and p_old, and no warp waits for another.  Same arithmetic and summation
-// order as k_pcg_pq.  A stage that does not arrive within the poll limit sets fl[5] (reported as
-// an error by the host) and the warp stops issuing copies.
-template <int WM, class T>
-constexpr int pq_stage_bytes() {  // per warp and stage
-  return 32 * WM * (int)(sizeof(T) + sizeof(int));
-}
-
-template <class T, int WM>
-__global__ void __launch_bounds__(kBlock) k_pcg_pq_staged(PcgArgsT<T> a, const T* pOld, T* pNew) {
-  extern __shared__ __align__(128) unsigned char stage[];
-  __shared__ double sm[32];
-  __shared__ __align__(8) unsigned long long bar[2 * (kBlock / 32)];
-  if (a.fl[0]) return;
-  constexpr int kValBytes = 32 * WM * (int)sizeof(T);
-  constexpr int kStage = pq_stage_bytes<WM, T>();
-  const int n = a.A.n;
-  const int nSlices = (n + 31) >> 5;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nWarps = gridDim.x * (kBlock / 32);
-  const int* so = a.A.sliceOff;
-  const bool first = a.fl[3] != 0;
-  const double beta = first ? 0.0 : a.sc[2];
-  unsigned long long* wb = bar + 2 * warp;
-  unsigned char* ws = stage + 2 * warp * kStage;
-  if (lane == 0) {
-    mbar_init(&wb[0], 1);
-    mbar_init(&wb[1], 1);
-    mbar_fence_init();
-  }
-  __syncwarp();
-  auto issue = [&](int sl, int st) {  // lane 0
-    const int e0 = __ldg(&so[sl]);
-    const unsigned cnt = (unsigned)(__ldg(&so[sl + 1]) - e0);
-    mbar_expect_tx(&wb[st], cnt * (unsigned)(sizeof(T) + sizeof(int)));
-    bulk_g2s(ws + st * kStage, a.A.val + e0, cnt * (unsigned)sizeof(T), &wb[st]);
-    bulk_g2s(ws + st * kStage + kValBytes, a.A.col + e0, cnt * (unsigned)sizeof(int), &wb[st]);
-  };
-  const int gw = blockIdx.x * (kBlock / 32) + warp;
-  if (lane == 0 && gw < nSlices) issue(gw, 0);
-  double acc[1] = {0};
-  bool failed = false, next = false;
-  int it = 0;
-  for (int sl = gw; sl < nSlices; sl += nWarps, ++it) {
-    const int st = it & 1;
-    next = sl + nWarps < nSlices;
-    if (lane == 0 && next) issue(sl + nWarps, st ^ 1);
-    const int r = (sl << 5) + lane;
-    const bool row = r < n;
-    // the row's own loads do not depend on the stage: issue them before the wait
-    const double zr = row ? (double)a.z[r] : 0.0;
-    const double por = row && !first ? (double)pOld[r] : 0.0;
-    const double dr = row ? (double)a.A.diag[r] : 0.0;
-    const int W = (__ldg(&so[sl + 1]) - __ldg(&so[sl])) >> 5;
-    const bool ok = mbar_wait(&wb[st], (unsigned)(it >> 1) & 1u);
-    if (row && ok) {
-      const T* sv = reinterpret_cast<const T*>(ws + st * kStage);
-      const int* sc = reinterpret_cast<const int*>(ws + st * kStage + kValBytes);
-      const double pr = first ? zr : (double)(T)(zr + beta * por);
-      double q = dr * pr;
-#pragma unroll
-      for (int k = 0; k < WM; ++k) {
-        if (k < W) {
-          const int c = sc[lane + (k << 5)];
-          const double v = (double)sv[lane + (k << 5)];
-          q += v * (first ? (double)a.z[c] : (double)(T)((double)a.z[c] + beta * (double)pOld[c]));
-        }
-      }
-      pNew[r] = (T)pr;
-      a.q[r] = (T)q;
-      acc[0] += pr * q;
-    }
-    // every lane is done with this stage before lane 0 refills it; a missed stage stops the warp
-    if (__any_sync(0xffffffffu, !ok)) {
-      failed = true;
-      break;
-    }
-  }
-  if (failed && lane == 0) {
-    a.fl[5] = 1;
-    // let the copies still in flight (this stage's, and the next slice's if issued) land before
-    // the block's shared memory is released; both waits are bounded
-    mbar_wait(&wb[it & 1], (unsigned)(it >> 1) & 1u);
-    if (next) mbar_wait(&wb[(it + 1) & 1], (unsigned)((it + 1) >> 1) & 1u);
   }
   if (grid_reduce<1>(acc, 0u, a.red, sm) && threadIdx.x == 0) {
     a.sc[5] = acc[0];
@@ -1388,24 +1291,7 @@ static void launch_pq(const LaunchCfg& lc, const PcgArgsT<T>& a, int it) {
   // and vectors halve in FP32
   const double by = lc.ab ? (sizeof(T) == 8 ? lc.ab->pcg_spmv() : 20.0 * lc.ab->C + 8.0 * lc.ab->nnzOff) : 0.0;
   ProfScope ps(lc, kKfPcgSpmv, by);
-  with_width(a.A.maxW, [&](auto W) {
-    constexpr int WM = W.value;
-    if constexpr (WM > 0) {
-      if (sell_staged(a.A)) {
-        constexpr int bytes = 2 * (kBlock / 32) * pq_stage_bytes<WM, T>();
-        auto kern = k_pcg_pq_staged<T, WM>;
-        if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        int grid = lc.rowBlocks;
-        if (lc.nSM > 0) {
-          const int wave = resident_blocks(reinterpret_cast<const void*>(kern), bytes) * lc.nSM;
-          if (wave > 0) grid = std::min(grid, wave);
-        }
-        kern<<<std::max(grid, 1), kBlock, bytes, lc.stream>>>(a, pOld, pNew);
-        return;
-      }
-    }
-    launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, WM>, a, pOld, pNew);
-  });
+  with_width(a.A.maxW, [&](auto W) { launch_rows(lc, lc.rowBlocks, k_pcg_pq<T, W.value>, a, pOld, pNew); });
 }
 
 // A solver loop as one graph: cond(h) (a one-thread kernel that sets the condition h), then a
