@@ -976,6 +976,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
   if (!out) return ANB_ERR_INVALID;
   *out = nullptr;
   if (!md || !prm) return ANB_ERR_INVALID;
+  CallerDevice keep;
   auto c = std::make_unique<anb_ctx>();
   auto clk = std::chrono::steady_clock::now();
   auto lap = [&](int k) {
@@ -1263,6 +1264,7 @@ int anb_create(const anb_mesh_desc* md, const anb_params* prm, anb_ctx** out) {
 
 void anb_destroy(anb_ctx* c) {
   if (!c) return;
+  CallerDevice keep;
   cudaSetDevice(c->prm.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   amg_release_graphs(c->amg);

@@ -174,8 +174,24 @@ constexpr int kScalRelchg = 56; // 6: momentum relative-change sums
 
 int fail(anb_ctx* c, const AnbError& e);
 
+// Every entry point leaves the caller's current device as it found it (the calls select the
+// context's device themselves).
+struct CallerDevice {
+  int dev = -1;
+  CallerDevice() {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+      cudaGetLastError();
+      dev = -1;
+    }
+  }
+  ~CallerDevice() {
+    if (dev >= 0) cudaSetDevice(dev);
+  }
+};
+
 template <class F>
 int guarded(anb_ctx* c, F&& f) {
+  CallerDevice keep;
   try {
     return f();
   } catch (const AnbError& e) {

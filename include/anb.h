@@ -17,6 +17,11 @@
  *     HYPRE error 256: warn and continue); other non-zero values are errors whose text is
  *     available from anb_last_error().  The library never calls exit() or abort().
  *   - A context is not thread-safe; distinct contexts are independent.
+ *   - Each call selects the context's device itself and leaves the caller's current device as it
+ *     found it.
+ *   - Cell fields cross the boundary through a pinned staging buffer of 4 x nCells doubles: the
+ *     host threads copy the caller's arrays into it in chunks, each chunk's DMA overlapping the
+ *     next copy, and a device kernel permutes between input and layout numbering.
  */
 #ifndef ANB_H
 #define ANB_H
