@@ -9,7 +9,7 @@
  * the file:line it follows (apps/generic_simple_v1/src/main.cu, "GSV1" below).  Pinning status:
  *   - geometry, LSQ gradient, Rhie-Chow, continuity, non-orthogonal flux, flux correction and
  *     patch forces are checked against the reference's own host functions compiled from
- *     /root/reference by oracle/build_ref.sh (tests/test_oracle_vs_reference.py);
+ *     the reference sources by oracle/build_ref.sh (tests/test_oracle_vs_reference.py);
  *   - the linear solves of the reference are HYPRE 3.0.0 (not vendored, not installable here):
  *     the oracle replaces them with deterministic FP64 Krylov solvers run to tight tolerance, so
  *     solver-level parity is unpinned and parity is checked on converged/tightly-solved fields.
