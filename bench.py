@@ -39,7 +39,7 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = dict(nx=200, ny=70, nz=70, jitter=0.15, seed=0, obstacle=True)
 PARAMS = dict(rho=1.0, mu=1e-3, u_relax=0.7, p_relax=0.3, n_nonorth_corr=2)
-KERNEL_FAMILY = 7  # ANB_KF_PCG_SPMV: the largest bandwidth-bound kernel of the step
+KERNEL_FAMILY = 7  # ANB_KF_PCG_SPMV: the PCG SpMV, a level-0 SELL kernel launched outside the V-cycle graph
 # DRAM bytes (read + write) per k_pcg_pq launch on this workload, from one launch of
 #   ANB_NO_LOOP_GRAPH=1 ncu --set full --clock-control none -k regex:"^k_pcg_pq$" -s 30 -c 1
 #       python bench.py --steps 2 --warmup 3 --no-cpu
